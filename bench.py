@@ -1,0 +1,320 @@
+#!/usr/bin/env python
+"""GCUPS of the PairHMM forward path on the uneven-length workload.
+
+One step = one batch of synthetic records with the shapes of the uneven-length
+configuration (20,000 regions, see gpupairhmm_b200/synth.py) through the
+engine's C ABI (pairhmm_compute_host): upload from pinned host memory,
+packing and work-list construction, the FP32 wavefront launches, the FP64
+pass, and the download of the scores.
+
+  value   cells / device time of the batch (CUDA events on the engine's stream
+          around everything after the upload: inputs resident in HBM)
+  e2e     cells / wall time of the blocking C-ABI call (host index, H2D, device
+          work, D2H), pinned host buffers
+  roofline  11 FP32 FLOP per DP cell / time of the FP32 wavefront launches,
+          against an FFMA peak measured on the same GPU in the same run
+
+Multi-GPU (torchrun): each rank runs its own replica on its own batch (weak
+scaling, no data-path collective); times are the max over ranks.
+
+--impl reference: the reference's own CPU forward (align_host, built from its
+sources into oracle/_ref/ with OpenMP over pairs) on all host cores, over a
+bounded sample of the same workload per step; falls back to the FP64 oracle
+port when the reference build is absent.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "GCUPS (PairHMM cells/s) at ≤1e-5 rel log10 err; p50/p99 region latency"
+FLOPS_PER_CELL = 11  # M: 5, I: 3, D: 3 (FMA = 2 FLOP)
+WORKLOAD = ("uneven lengths: 20,000 regions, R ~ lognormal(median 40, sigma 1.0) clipped 1-400, "
+            "H ~ U{1..16}, read length {100,150,250} (.3/.5/.2) minus U{0..30}, "
+            "haplotype = read + U{50..400}, base quality U{10..40}, ins/del 40, gcp 10")
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--mode", choices=["engine", "plain"], default="engine")
+    ap.add_argument("--regions", type=int, default=20000)
+    ap.add_argument("--seed", type=int, default=1)
+    ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU baseline sample size (seconds of work)")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--accuracy-pairs", type=int, default=3000)
+    return ap.parse_args()
+
+
+# ----------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi samples every 200 ms while the timed region runs."""
+
+    FIELDS = ("index,uuid,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, uuid: str | None):
+        self.uuid = uuid
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(prefix="clocks_", suffix=".csv")
+        os.close(fd)
+        cmd = ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200"]
+        if self.uuid:
+            cmd += ["-i", self.uuid]
+        try:
+            self.proc = subprocess.Popen(cmd, stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        rows = []
+        for ln in Path(self.path).read_text().splitlines():
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) >= 10:
+                rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        sm = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        mx = [float(r[3]) for r in rows if r[3].replace(".", "").isdigit()]
+        pw = [float(r[4]) for r in rows if r[4].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[6 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "power_w_median": statistics.median(pw) if pw else None, "reasons": reasons,
+                "samples": len(rows)}
+
+
+# ----------------------------------------------------------------- helpers
+def traffic_per_cell():
+    """DRAM bytes per DP cell of the FP32 wavefront from the committed ncu
+    summary (profiles/fp32_wavefront_traffic.json), or None."""
+    p = ROOT / "profiles" / "fp32_wavefront_traffic.json"
+    if not p.exists():
+        return None
+    try:
+        return float(json.loads(p.read_text())["dram_bytes_per_cell"])
+    except Exception:
+        return None
+
+
+def sample_records(batch, target_cells: int, rng: np.random.Generator):
+    """Contiguous records from a random start with about target_cells cells."""
+    from gpupairhmm_b200 import replicas
+    c = replicas.record_cells(batch)
+    start = int(rng.integers(0, max(1, batch.num_records - 1)))
+    cs = np.cumsum(c[start:])
+    end = start + int(np.searchsorted(cs, target_cells)) + 1
+    end = min(end, batch.num_records)
+    return batch.select_records(start, end), end - start
+
+
+def cpu_rate(fn, batch, target_seconds: float, rng):
+    """Time fn over a sample sized for about target_seconds; returns (GCUPS, sample text)."""
+    probe, _ = sample_records(batch, int(2e8), rng)
+    t = time.perf_counter()
+    fn(probe)
+    rate = probe.cells() / max(time.perf_counter() - t, 1e-6)
+    sub, nrec = sample_records(batch, int(rate * target_seconds), rng)
+    t = time.perf_counter()
+    fn(sub)
+    dt = time.perf_counter() - t
+    return sub.cells() / dt / 1e9, f"{nrec} consecutive records, {sub.num_pairs} pairs, {sub.cells()} cells, {dt:.1f} s"
+
+
+def accuracy(batch, scores, n, rng):
+    import oracle
+    pick = np.sort(rng.choice(batch.num_records, size=min(batch.num_records, max(1, n // 40)), replace=False))
+    from gpupairhmm_b200 import replicas, synth
+    po = replicas.pair_offsets(batch)
+    parts = [batch.select_records(int(g), int(g) + 1) for g in pick]
+    sub = synth.concat(parts)
+    want = oracle.batch_log10(sub)
+    got = np.concatenate([scores[po[g]:po[g + 1]] for g in pick]).astype(np.float64)
+    err = np.abs(got - want)
+    rel = err / np.maximum(np.abs(want), 1e-30)
+    return {"sample_pairs": int(len(want)), "max_abs_log10": float(err.max()), "mean_abs_log10": float(err.mean()),
+            "max_rel_log10": float(rel.max()), "within_1e-5_rel": bool(np.all(err <= 1e-5 * np.abs(want) + 1e-6))}
+
+
+# ----------------------------------------------------------------- arms
+def run_reference(args, cfg):
+    """The reference's own CPU implementation, all host threads."""
+    import oracle
+    from gpupairhmm_b200 import synth
+    batch = synth.config1(seed=args.seed, regions=args.regions)
+    rng = np.random.default_rng(1234)
+    ref_ok = oracle.ref_cpu() is not None
+    fn = (lambda b: oracle.ref_batch_log10(b)) if ref_ok else (lambda b: oracle.batch_log10(b))
+    kind = "reference" if ref_ok else "port"
+    cores = os.cpu_count() or 1
+    per_step = max(2.0, min(12.0, 120.0 / max(1, args.steps + args.warmup)))
+    # size one step's sample from a probe, then run warmup + steps
+    probe, _ = sample_records(batch, int(2e8), rng)
+    t = time.perf_counter()
+    fn(probe)
+    rate = probe.cells() / max(time.perf_counter() - t, 1e-6)
+    sub, nrec = sample_records(batch, int(rate * per_step), rng)
+    for _ in range(args.warmup):
+        fn(sub)
+    t = time.perf_counter()
+    for _ in range(args.steps):
+        fn(sub)
+    dt = time.perf_counter() - t
+    value = sub.cells() * args.steps / dt / 1e9
+    sample = (f"{nrec} consecutive records of the workload per step ({sub.num_pairs} pairs, {sub.cells()} cells); "
+              f"{'reference align_host (gpuworker.cuh:1022-1098), FP32 cells, OpenMP over pairs' if ref_ok else 'FP64 oracle port'}")
+    line = {"impl": "reference", "metric": METRIC, "value": round(value, 4), "unit": "GCUPS", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(dt / args.steps * 1e3, 3),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp32",
+            "data": "synthetic", "config": cfg,
+            "cpu_baseline": {"value": round(value, 4), "unit": "GCUPS", "cores": cores, "kind": kind,
+                             "sample": sample},
+            "e2e": {"value": round(value, 4), "unit": "GCUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, cfg, rank, world, local_rank):
+    import torch
+    import gpupairhmm_b200 as g
+    from gpupairhmm_b200 import synth
+
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local_rank))
+
+    batch = synth.config1(seed=args.seed + rank, regions=args.regions)
+    cells = batch.cells()
+    pinned = batch.pin()
+    mode = g.MODE_PLAIN if args.mode == "plain" else g.MODE_ENGINE
+    engine = g.Engine(device=local_rank, mode=mode)
+    peak = g.probe_fp32_peak(local_rank, 100)
+    scores = np.empty(batch.num_pairs, dtype=np.float32)
+    for _ in range(args.warmup):
+        engine.compute(pinned, out=scores)
+
+    props = torch.cuda.get_device_properties(local_rank)
+    uuid = str(getattr(props, "uuid", "") or "")
+    uuid = ("GPU-" + uuid) if uuid and not uuid.startswith("GPU-") else (uuid or None)
+    sampler = ClockSampler(uuid)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    sampler.start()
+    time.sleep(0.25)
+    dev_ms = fp32_ms = prep_ms = fp64_ms = 0.0
+    launches = h2d = d2h = rescued = 0
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        engine.compute(pinned, out=scores)
+        st = engine.stats()
+        dev_ms += st.device_ms
+        fp32_ms += st.fp32_ms
+        prep_ms += st.prep_ms
+        fp64_ms += st.fp64_ms
+        launches += st.launches
+        h2d += st.h2d_bytes
+        d2h += st.d2h_bytes
+        rescued = st.rescued
+    torch.cuda.synchronize()
+    t1 = time.perf_counter()
+    clocks = sampler.stop()
+    if dist:
+        dist.barrier()
+    wall = t1 - t0
+    times = np.array([wall, dev_ms / 1e3, fp32_ms / 1e3], dtype=np.float64)
+    if dist:
+        tt = torch.tensor(times, device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        times = tt.cpu().numpy()
+    wall, dev_s, fp32_s = (float(x) for x in times)
+    total_cells = cells * args.steps * world
+
+    if rank == 0:
+        value = total_cells / dev_s / 1e9
+        e2e = total_cells / wall / 1e9
+        achieved = FLOPS_PER_CELL * cells * args.steps / fp32_s / 1e12
+        tpc = traffic_per_cell()
+        n_fp32_launches = max(1, launches // max(1, args.steps) - 7)
+        rng = np.random.default_rng(99)
+        line = {
+            "metric": METRIC, "value": round(value, 3), "unit": "GCUPS", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(dev_s / args.steps * 1e3, 3), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "fp32", "data": "synthetic",
+            "config": dict(cfg, pairs=batch.num_pairs, cells=cells, rescued_fp64=rescued,
+                           parallelism=f"replicas{world}"),
+            "e2e": {"value": round(e2e, 3), "unit": "GCUPS", "h2d_bytes_per_step": h2d // args.steps,
+                    "d2h_bytes_per_step": d2h // args.steps, "ms_per_step": round(wall / args.steps * 1e3, 3)},
+            "gpu_launches": int(launches),
+            "roofline": {"bound": "fp32", "achieved": round(achieved, 3), "peak": round(peak, 3),
+                         "unit": "TFLOP/s", "frac": round(achieved / peak, 4),
+                         "traffic": (round(tpc * cells / n_fp32_launches) if tpc else None),
+                         "peak_source": "FFMA throughput measured in this run on this GPU (no FP32 entry in "
+                                        "the driver's peak file)",
+                         "flop_per_cell": FLOPS_PER_CELL, "instruction_mix_ceiling": round(11 / 14, 4),
+                         "kernel": "fp32_bucket_kernel (all length buckets)",
+                         "stage_ms_per_step": {"prep": round(prep_ms / args.steps, 3),
+                                               "fp32": round(fp32_ms / args.steps, 3),
+                                               "fp64": round(fp64_ms / args.steps, 3)}},
+            "clocks": clocks,
+            "accuracy": accuracy(batch, scores, args.accuracy_pairs, rng),
+        }
+        if world == 1 and not args.no_cpu_baseline:
+            import oracle
+            gc, desc = cpu_rate(lambda b: oracle.batch_log10(b), batch, args.cpu_seconds, rng)
+            line["cpu_baseline"] = {"value": round(gc, 4), "unit": "GCUPS", "cores": os.cpu_count() or 1,
+                                    "kind": "port", "sample": desc + "; FP64 oracle, OpenMP over pairs"}
+        print(json.dumps(line), flush=True)
+    engine.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse_args()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    cfg = {"workload": WORKLOAD, "regions": args.regions, "seed": args.seed, "sigma": 1.0, "mode": args.mode,
+           "l2": "inputs larger than L2 (packed batch ~1 GB vs 126 MB)"}
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        run_reference(args, cfg)
+        return
+    run_ours(args, cfg, rank, world, local_rank)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,287 @@
+// extern "C" boundary: no C++ exceptions or types cross it.
+#include <cstring>
+#include <memory>
+#include <new>
+
+#include "engine.hpp"
+#include "records.hpp"
+#include "serving.hpp"
+
+struct pairhmm_records {
+    phmm::HostBatch batch;
+};
+
+struct pairhmm_engine {
+    std::unique_ptr<phmm::Engine> engine;
+    std::unique_ptr<phmm::ServingQueue> serving;
+    std::string error;
+};
+
+namespace {
+
+template <class F>
+pairhmm_status_t guarded(pairhmm_engine* h, F&& f) {
+    try {
+        return f();
+    } catch (const std::bad_alloc&) {
+        if (h) h->error = "host allocation failed";
+        return PAIRHMM_ERR_OUT_OF_MEMORY;
+    } catch (const std::exception& e) {
+        if (h) h->error = e.what();
+        return PAIRHMM_ERR_CUDA;
+    } catch (...) {
+        if (h) h->error = "unknown exception";
+        return PAIRHMM_ERR_CUDA;
+    }
+}
+
+pairhmm_status_t finish(pairhmm_engine* h, pairhmm_status_t s) {
+    if (s != PAIRHMM_OK) h->error = h->engine->last_error();
+    else h->error.clear();
+    return s;
+}
+
+}  // namespace
+
+extern "C" {
+
+void pairhmm_default_options(pairhmm_options_t* o) {
+    if (!o) return;
+    o->device = 0;
+    o->mode = PAIRHMM_MODE_ENGINE;
+    o->fp64_rescue = 1;
+    o->use_graphs = 1;
+    o->device_budget_bytes = 0;
+}
+
+pairhmm_status_t pairhmm_engine_create(const pairhmm_options_t* opts, pairhmm_engine_t** out) {
+    if (!out) return PAIRHMM_ERR_INVALID_ARGUMENT;
+    *out = nullptr;
+    pairhmm_options_t o;
+    pairhmm_default_options(&o);
+    if (opts) o = *opts;
+    if (o.mode != PAIRHMM_MODE_ENGINE && o.mode != PAIRHMM_MODE_PLAIN) return PAIRHMM_ERR_INVALID_ARGUMENT;
+    auto* h = new (std::nothrow) pairhmm_engine;
+    if (!h) return PAIRHMM_ERR_OUT_OF_MEMORY;
+    pairhmm_status_t s = guarded(h, [&] {
+        h->engine = std::make_unique<phmm::Engine>(o);
+        return h->engine->init();
+    });
+    if (s != PAIRHMM_OK) {
+        delete h;
+        return s;
+    }
+    *out = h;
+    return PAIRHMM_OK;
+}
+
+pairhmm_status_t pairhmm_engine_destroy(pairhmm_engine_t* h) {
+    if (!h) return PAIRHMM_ERR_INVALID_ARGUMENT;
+    pairhmm_status_t s = guarded(h, [&] {
+        h->serving.reset();
+        h->engine.reset();
+        return PAIRHMM_OK;
+    });
+    delete h;
+    return s;
+}
+
+pairhmm_status_t pairhmm_compute_host(pairhmm_engine_t* h, const pairhmm_batch_t* batch, float* scores) {
+    if (!h || !batch) return PAIRHMM_ERR_INVALID_ARGUMENT;
+    return guarded(h, [&] { return finish(h, h->engine->compute_host(*batch, scores)); });
+}
+
+pairhmm_status_t pairhmm_compute_device(pairhmm_engine_t* h, const pairhmm_batch_t* batch, int32_t max_read_length,
+                                        int32_t max_hap_length, float* scores, void* stream) {
+    if (!h || !batch) return PAIRHMM_ERR_INVALID_ARGUMENT;
+    return guarded(h, [&] {
+        return finish(h, h->engine->compute_device(*batch, max_read_length, max_hap_length, scores,
+                                                   static_cast<cudaStream_t>(stream)));
+    });
+}
+
+pairhmm_status_t pairhmm_get_stats(pairhmm_engine_t* h, pairhmm_stats_t* stats) {
+    if (!h || !stats) return PAIRHMM_ERR_INVALID_ARGUMENT;
+    *stats = h->engine->stats();
+    return PAIRHMM_OK;
+}
+
+pairhmm_status_t pairhmm_submit(pairhmm_engine_t* h, const pairhmm_batch_t* region, uint64_t* ticket) {
+    if (!h || !region || !ticket) return PAIRHMM_ERR_INVALID_ARGUMENT;
+    return guarded(h, [&] {
+        if (!h->serving) h->serving = std::make_unique<phmm::ServingQueue>(*h->engine);
+        pairhmm_status_t s = h->serving->submit(*region, ticket);
+        if (s != PAIRHMM_OK) h->error = h->serving->last_error();
+        return s;
+    });
+}
+
+pairhmm_status_t pairhmm_poll(pairhmm_engine_t* h, uint64_t ticket, int32_t* done) {
+    if (!h || !done) return PAIRHMM_ERR_INVALID_ARGUMENT;
+    return guarded(h, [&] {
+        if (!h->serving) return PAIRHMM_ERR_NOT_FOUND;
+        pairhmm_status_t s = h->serving->poll(ticket, done);
+        if (s != PAIRHMM_OK) h->error = h->serving->last_error();
+        return s;
+    });
+}
+
+pairhmm_status_t pairhmm_drain(pairhmm_engine_t* h, uint64_t ticket, float* scores, int64_t num_scores,
+                               int32_t timeout_ms) {
+    if (!h || (!scores && num_scores > 0)) return PAIRHMM_ERR_INVALID_ARGUMENT;
+    return guarded(h, [&] {
+        if (!h->serving) return PAIRHMM_ERR_NOT_FOUND;
+        pairhmm_status_t s = h->serving->drain(ticket, scores, num_scores, timeout_ms);
+        if (s != PAIRHMM_OK) h->error = h->serving->last_error();
+        return s;
+    });
+}
+
+pairhmm_status_t pairhmm_region_latency_ms(pairhmm_engine_t* h, uint64_t ticket, double* ms) {
+    if (!h || !ms) return PAIRHMM_ERR_INVALID_ARGUMENT;
+    return guarded(h, [&] {
+        if (!h->serving) return PAIRHMM_ERR_NOT_FOUND;
+        pairhmm_status_t s = h->serving->latency(ticket, ms);
+        if (s != PAIRHMM_OK) h->error = h->serving->last_error();
+        return s;
+    });
+}
+
+const char* pairhmm_status_string(pairhmm_status_t s) {
+    switch (s) {
+        case PAIRHMM_OK: return "ok";
+        case PAIRHMM_ERR_INVALID_ARGUMENT: return "invalid argument";
+        case PAIRHMM_ERR_CUDA: return "CUDA error";
+        case PAIRHMM_ERR_OUT_OF_MEMORY: return "out of memory";
+        case PAIRHMM_ERR_BUDGET: return "region exceeds the device budget";
+        case PAIRHMM_ERR_NOT_FOUND: return "unknown ticket";
+        case PAIRHMM_ERR_TIMEOUT: return "timed out";
+        case PAIRHMM_ERR_UNSUPPORTED: return "unsupported";
+        case PAIRHMM_ERR_BUSY: return "busy";
+    }
+    return "unknown status";
+}
+
+const char* pairhmm_last_error(const pairhmm_engine_t* h) { return h ? h->error.c_str() : ""; }
+
+pairhmm_status_t pairhmm_batch_counts(const pairhmm_batch_t* batch, int64_t* pairs, int64_t* cells) {
+    if (!batch) return PAIRHMM_ERR_INVALID_ARGUMENT;
+    phmm::BatchIndex x;
+    std::string err;
+    pairhmm_status_t s;
+    try {
+        s = phmm::Engine::build_index(*batch, {{1 << 30, 32, 32, true}}, x, err);
+    } catch (...) {
+        return PAIRHMM_ERR_OUT_OF_MEMORY;
+    }
+    if (s != PAIRHMM_OK) return s;
+    if (pairs) *pairs = x.num_pairs;
+    if (cells) *cells = x.cells;
+    return PAIRHMM_OK;
+}
+
+pairhmm_status_t pairhmm_records_parse(const char* text, int64_t length, pairhmm_records_t** out) {
+    if (!out || (!text && length > 0) || length < 0) return PAIRHMM_ERR_INVALID_ARGUMENT;
+    *out = nullptr;
+    try {
+        auto r = std::make_unique<pairhmm_records>();
+        std::string err;
+        if (!phmm::parse_records(std::string(text ? text : "", (size_t)length), r->batch, err))
+            return PAIRHMM_ERR_INVALID_ARGUMENT;
+        *out = r.release();
+        return PAIRHMM_OK;
+    } catch (...) {
+        return PAIRHMM_ERR_OUT_OF_MEMORY;
+    }
+}
+
+pairhmm_status_t pairhmm_records_view(const pairhmm_records_t* r, pairhmm_batch_t* view, int64_t* num_pairs) {
+    if (!r || !view) return PAIRHMM_ERR_INVALID_ARGUMENT;
+    *view = r->batch.view();
+    if (num_pairs) *num_pairs = r->batch.pairs;
+    return PAIRHMM_OK;
+}
+
+pairhmm_status_t pairhmm_records_format(const pairhmm_records_t* r, const float* scores, char* buf,
+                                        int64_t capacity, int64_t* length) {
+    if (!r || !length || (!scores && r->batch.pairs > 0)) return PAIRHMM_ERR_INVALID_ARGUMENT;
+    try {
+        std::string text;
+        phmm::format_scores(r->batch, scores, text);
+        *length = (int64_t)text.size();
+        if (buf && capacity > (int64_t)text.size()) {
+            std::memcpy(buf, text.data(), text.size());
+            buf[text.size()] = '\0';
+        }
+        return PAIRHMM_OK;
+    } catch (...) {
+        return PAIRHMM_ERR_OUT_OF_MEMORY;
+    }
+}
+
+void pairhmm_records_free(pairhmm_records_t* r) { delete r; }
+
+const char* pairhmm_version(void) { return "pairhmm_b200 0.1.0 (sm_100a)"; }
+
+pairhmm_status_t pairhmm_set_tile_table(pairhmm_engine_t* h, const int32_t* max_len, const int32_t* group,
+                                        const int32_t* regs, const int32_t* multi_tile, int32_t n) {
+    if (!h || !max_len || !group || !regs || !multi_tile || n <= 0) return PAIRHMM_ERR_INVALID_ARGUMENT;
+    return guarded(h, [&] {
+        std::vector<phmm::TileRule> rules(n);
+        for (int i = 0; i < n; ++i) rules[i] = {max_len[i], group[i], regs[i], multi_tile[i] != 0};
+        return finish(h, h->engine->set_tile_table(rules));
+    });
+}
+
+pairhmm_status_t pairhmm_get_tile_table(pairhmm_engine_t* h, int32_t* max_len, int32_t* group, int32_t* regs,
+                                        int32_t* multi_tile, int32_t capacity, int32_t* n) {
+    if (!h || !n) return PAIRHMM_ERR_INVALID_ARGUMENT;
+    const auto& r = h->engine->tile_table();
+    *n = (int32_t)r.size();
+    if (capacity < (int32_t)r.size() || !max_len || !group || !regs || !multi_tile) return PAIRHMM_OK;
+    for (size_t i = 0; i < r.size(); ++i) {
+        max_len[i] = r[i].max_len;
+        group[i] = r[i].G;
+        regs[i] = r[i].R;
+        multi_tile[i] = r[i].multi_tile ? 1 : 0;
+    }
+    return PAIRHMM_OK;
+}
+
+pairhmm_status_t pairhmm_probe_fp32_peak(int32_t device, int32_t milliseconds, double* tflops) {
+    if (!tflops || milliseconds <= 0) return PAIRHMM_ERR_INVALID_ARGUMENT;
+    if (cudaSetDevice(device) != cudaSuccess) return PAIRHMM_ERR_CUDA;
+    cudaDeviceProp prop{};
+    if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) return PAIRHMM_ERR_CUDA;
+    float* out = nullptr;
+    cudaStream_t s = nullptr;
+    cudaEvent_t a = nullptr, b = nullptr;
+    if (cudaMalloc(&out, 16) != cudaSuccess) return PAIRHMM_ERR_OUT_OF_MEMORY;
+    cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    const int grid = prop.multiProcessorCount * 8;  // 8 x 256 threads per SM
+    int iters = 1000;
+    double best = 0.0;
+    pairhmm_status_t st = PAIRHMM_OK;
+    // grow until one launch takes the requested time, then keep the best of 3
+    for (int rep = 0; rep < 12 && st == PAIRHMM_OK; ++rep) {
+        cudaEventRecord(a, s);
+        if (phmm::launch_ffma_peak(out, grid, iters, s) != cudaSuccess) st = PAIRHMM_ERR_CUDA;
+        cudaEventRecord(b, s);
+        if (cudaEventSynchronize(b) != cudaSuccess) st = PAIRHMM_ERR_CUDA;
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, a, b);
+        const double flops = (double)grid * 256 * (double)iters * 128.0 * 2.0;
+        if (ms > 0.f) best = std::max(best, flops / (ms * 1e-3) / 1e12);
+        if (ms < milliseconds && rep < 9) iters = (int)std::min<double>(iters * 2.0, 4e8);
+    }
+    *tflops = best;
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    cudaStreamDestroy(s);
+    cudaFree(out);
+    return st;
+}
+
+}  // extern "C"

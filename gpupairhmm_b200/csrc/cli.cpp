@@ -1,0 +1,222 @@
+// Command-line front end with the reference's flags (main.cu:47-75) and its
+// three-stage pipeline (main.cu:7-27): a parser thread, a GPU thread and a
+// writer thread pass queue_depth batch buffers around in a ring.
+//
+//   pairhmm_b200 --inputfile in.txt --outputfile out.txt
+//                [--fileBatchsize N] [--transferBatchsize N] [--queue_depth N]
+//                [--verbose] [--checkResults] [--mode engine|plain]
+//
+// fileBatchsize: minimum pairs per parsed batch; transferBatchsize: minimum
+// pairs per engine call inside a batch; a value <= 0 means unlimited
+// (main.cu:77-83).  Defaults follow the reference's code: 1,000,000 and
+// 10,000,000 (common.cuh:19-20).  --checkResults is accepted and, as in the
+// reference, has no effect.
+#include <atomic>
+#include <chrono>
+#include <condition_variable>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <iostream>
+#include <limits>
+#include <memory>
+#include <mutex>
+#include <queue>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "../../include/pairhmm_b200.h"
+#include "records.hpp"
+
+namespace {
+
+struct Options {
+    bool checkResults = false;
+    bool verbose = false;
+    int64_t transferBatchsize = 1000000;
+    int64_t fileBatchsize = 10000000;
+    int queue_depth = 3;
+    int mode = PAIRHMM_MODE_ENGINE;
+    std::string inputfile;
+    std::string outputfile;
+};
+
+struct PipelineData {
+    phmm::HostBatch batch;
+    std::vector<float> scores;
+};
+
+template <class T>
+class Queue {
+public:
+    void push(T v) {
+        std::lock_guard<std::mutex> lk(m_);
+        q_.push(v);
+        cv_.notify_one();
+    }
+    T pop() {
+        std::unique_lock<std::mutex> lk(m_);
+        cv_.wait(lk, [&] { return !q_.empty(); });
+        T v = q_.front();
+        q_.pop();
+        return v;
+    }
+
+private:
+    std::mutex m_;
+    std::condition_variable cv_;
+    std::queue<T> q_;
+};
+
+std::atomic<bool> g_failed{false};
+
+void die(const std::string& msg) {
+    std::cerr << msg << "\n";
+    std::exit(EXIT_FAILURE);  // as the reference's workers do (gpuworker.cu:33-39)
+}
+
+void parser_thread(const Options& o, Queue<PipelineData*>* in, Queue<PipelineData*>* out) {
+    phmm::RecordReader reader(o.inputfile);
+    if (!reader.ok()) die(reader.error());
+    for (;;) {
+        PipelineData* d = in->pop();
+        d->batch.clear();
+        bool eof = false;
+        if (!reader.next(d->batch, o.fileBatchsize, eof)) die("parse error: " + reader.error());
+        if (d->batch.num_records() > 0) out->push(d);
+        else in->push(d);
+        if (eof) break;
+    }
+    out->push(nullptr);
+}
+
+void gpu_thread(const Options& o, Queue<PipelineData*>* in, Queue<PipelineData*>* out, double* seconds,
+                int64_t* cells_total) {
+    pairhmm_options_t eo;
+    pairhmm_default_options(&eo);
+    eo.mode = o.mode;
+    pairhmm_engine_t* eng = nullptr;
+    pairhmm_status_t st = pairhmm_engine_create(&eo, &eng);
+    if (st != PAIRHMM_OK) die(std::string("engine: ") + pairhmm_status_string(st));
+    for (;;) {
+        PipelineData* d = in->pop();
+        if (!d) break;
+        const auto t0 = std::chrono::steady_clock::now();
+        phmm::HostBatch& b = d->batch;
+        d->scores.resize((size_t)std::max<int64_t>(b.pairs, 1));
+        // transfer chunks: consecutive records with at least transferBatchsize pairs
+        int64_t g = 0, read0 = 0, hap0 = 0, pair0 = 0;
+        const int64_t ng = b.num_records();
+        while (g < ng) {
+            int64_t g1 = g, reads = 0, haps = 0, pairs = 0;
+            while (g1 < ng && (pairs < o.transferBatchsize || g1 == g)) {
+                reads += b.reads_per_record[g1];
+                haps += b.haps_per_record[g1];
+                pairs += (int64_t)b.reads_per_record[g1] * b.haps_per_record[g1];
+                ++g1;
+            }
+            pairhmm_batch_t v = b.view();
+            v.num_records = g1 - g;
+            v.reads_per_record += g;
+            v.haps_per_record += g;
+            v.read_offsets += read0;
+            v.read_lengths += read0;
+            v.hap_offsets += hap0;
+            v.hap_lengths += hap0;
+            st = pairhmm_compute_host(eng, &v, d->scores.data() + pair0);
+            if (st != PAIRHMM_OK)
+                die(std::string("compute: ") + pairhmm_status_string(st) + ": " + pairhmm_last_error(eng));
+            pairhmm_stats_t s{};
+            pairhmm_get_stats(eng, &s);
+            *cells_total += s.cells;
+            if (o.verbose)
+                std::cout << "chunk: " << s.pairs << " pairs, " << s.rescued << " rescued, " << s.device_ms
+                          << " ms device\n";
+            g = g1;
+            read0 += reads;
+            hap0 += haps;
+            pair0 += pairs;
+        }
+        *seconds += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        out->push(d);
+    }
+    out->push(nullptr);
+    pairhmm_engine_destroy(eng);
+}
+
+void writer_thread(const Options& o, Queue<PipelineData*>* in, Queue<PipelineData*>* out) {
+    // an empty name writes to stdout; /dev/null skips formatting (output_writer_worker.cu:36-61)
+    const bool no_output = o.outputfile == "/dev/null";
+    FILE* f = stdout;
+    if (!o.outputfile.empty() && !no_output) {
+        f = std::fopen(o.outputfile.c_str(), "wb");
+        if (!f) die("could not open file " + o.outputfile);
+    }
+    std::string text;
+    for (;;) {
+        PipelineData* d = in->pop();
+        if (!d) break;
+        if (!no_output) {
+            text.clear();
+            phmm::format_scores(d->batch, d->scores.data(), text);
+            if (std::fwrite(text.data(), 1, text.size(), f) != text.size()) die("write failed");
+        }
+        d->batch.clear();
+        out->push(d);
+    }
+    if (f != stdout) std::fclose(f);
+    else std::fflush(stdout);
+}
+
+}  // namespace
+
+int main(int argc, char** argv) {
+    Options o;
+    for (int x = 1; x < argc; ++x) {
+        const std::string a = argv[x];
+        auto val = [&](const char* name) -> std::string {
+            if (x + 1 >= argc) die(std::string("missing value for ") + name);
+            return argv[++x];
+        };
+        if (a == "--inputfile") o.inputfile = val("--inputfile");
+        else if (a == "--outputfile") o.outputfile = val("--outputfile");
+        else if (a == "--transferBatchsize") o.transferBatchsize = std::atoll(val("--transferBatchsize").c_str());
+        else if (a == "--fileBatchsize") o.fileBatchsize = std::atoll(val("--fileBatchsize").c_str());
+        else if (a == "--queue_depth") o.queue_depth = std::atoi(val("--queue_depth").c_str());
+        else if (a == "--checkResults") o.checkResults = true;
+        else if (a == "--verbose") o.verbose = true;
+        else if (a == "--mode") {
+            const std::string m = val("--mode");
+            if (m == "plain") o.mode = PAIRHMM_MODE_PLAIN;
+            else if (m == "engine") o.mode = PAIRHMM_MODE_ENGINE;
+            else die("--mode must be engine or plain");
+        }
+    }
+    if (o.transferBatchsize <= 0) o.transferBatchsize = std::numeric_limits<int64_t>::max();
+    if (o.fileBatchsize <= 0) o.fileBatchsize = std::numeric_limits<int64_t>::max();
+    if (o.queue_depth < 1) o.queue_depth = 1;
+    std::cout << "options.inputfile = " << o.inputfile << "\n";
+    std::cout << "options.outputfile = " << o.outputfile << "\n";
+    std::cout << "options.transferBatchsize = " << o.transferBatchsize << "\n";
+    std::cout << "options.verbose = " << o.verbose << "\n";
+    std::cout << "options.fileBatchsize = " << o.fileBatchsize << "\n";
+
+    Queue<PipelineData*> to_parser, to_gpu, to_writer;
+    std::vector<std::unique_ptr<PipelineData>> buffers;
+    for (int i = 0; i < o.queue_depth; ++i) {
+        buffers.push_back(std::make_unique<PipelineData>());
+        to_parser.push(buffers.back().get());
+    }
+    double seconds = 0.0;
+    int64_t cells = 0;
+    std::thread tp(parser_thread, std::cref(o), &to_parser, &to_gpu);
+    std::thread tg(gpu_thread, std::cref(o), &to_gpu, &to_writer, &seconds, &cells);
+    std::thread tw(writer_thread, std::cref(o), &to_writer, &to_parser);
+    tp.join();
+    tg.join();
+    tw.join();
+    const double gcups = seconds > 0 ? cells / 1e9 / seconds : 0.0;
+    std::cout << "Batch processing time: " << seconds << "s (" << gcups << " GCUPS)\n";
+    return 0;
+}

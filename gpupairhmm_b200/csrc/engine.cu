@@ -1,0 +1,664 @@
+// Host-side engine: batch validation and indexing, device buffers, the
+// per-batch launch sequence and its CUDA-graph replay.
+//
+// Launch sequence of one batch (all on one stream, replayed as one graph):
+//   pack_reads / pack_haps      caller SoA -> packed HBM layout
+//   bin_count, hist_scan,
+//   schedule, bin_scatter       sorted work list + per-bucket task ranges
+//   fp32_bucket_kernel<G,R,MT>  one launch per non-empty length bucket
+//   fp64_rescue_kernel          pairs flagged by the FP32 pass
+// Compared with the reference executor (gpuworker.cuh:559-973) there is no
+// device-to-host synchronisation inside a batch: the host derives bucket sizes
+// from the record structure it already holds, and the kernels read their task
+// ranges from device memory.
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+
+#include "engine.hpp"
+
+namespace phmm {
+
+namespace {
+
+constexpr int64_t kScratchBudget = int64_t(4) << 30;  // border scratch cap per batch
+
+std::vector<TileRule> engine_default_rules() {
+    // Tile per read-length bucket for the persistent engine.  Replaced at
+    // start-up by the tuned table when one is provided.
+    return {
+        {32, 4, 8, false},     {48, 4, 12, false},    {64, 4, 16, false},    {80, 4, 20, false},
+        {96, 4, 24, false},    {112, 4, 28, false},   {128, 4, 32, false},   {160, 8, 20, false},
+        {192, 8, 24, false},   {224, 8, 28, false},   {256, 8, 32, false},   {320, 16, 20, false},
+        {384, 16, 24, false},  {448, 16, 28, false},  {512, 16, 32, false},  {640, 32, 20, false},
+        {768, 32, 24, false},  {896, 32, 28, false},  {1024, 32, 32, false}, {1280, 32, 20, true},
+        {1536, 32, 24, true},  {1792, 32, 28, true},  {2048, 32, 32, true},  {1 << 30, 32, 32, true},
+    };
+}
+
+std::vector<TileRule> plain_rules() {
+    // The reference's generic single-tile table (tuningconfigs.hpp:33-57) and
+    // its multi-tile configuration for longer reads (gpuworker.cuh:189-194).
+    return {
+        {16, 4, 4, false},     {32, 4, 8, false},     {48, 4, 12, false},    {64, 4, 16, false},
+        {80, 4, 20, false},    {96, 4, 24, false},    {112, 4, 28, false},   {128, 4, 32, false},
+        {160, 8, 20, false},   {192, 8, 24, false},   {224, 8, 28, false},   {256, 8, 32, false},
+        {320, 16, 20, false},  {384, 16, 24, false},  {448, 16, 28, false},  {512, 16, 32, false},
+        {640, 32, 20, false},  {768, 32, 24, false},  {896, 32, 28, false},  {1024, 32, 32, false},
+        {1 << 30, 32, 16, true},
+    };
+}
+
+inline int64_t round_up(int64_t x, int64_t m) { return (x + m - 1) / m * m; }
+
+int bucket_of_host(int L, const std::vector<TileRule>& rules) {
+    int b = 0;
+    const int nb = (int)rules.size();
+    while (b < nb - 1 && L > rules[b].max_len) ++b;
+    return b;
+}
+
+}  // namespace
+
+cudaError_t DevBuf::ensure(size_t bytes) {
+    if (bytes <= cap && ptr) return cudaSuccess;
+    release();
+    size_t want = std::max<size_t>(bytes + bytes / 4, 256);
+    cudaError_t e = cudaMalloc(&ptr, want);
+    if (e != cudaSuccess) {
+        ptr = nullptr;
+        cap = 0;
+        return e;
+    }
+    cap = want;
+    return cudaSuccess;
+}
+
+void DevBuf::release() {
+    if (ptr) cudaFree(ptr);
+    ptr = nullptr;
+    cap = 0;
+}
+
+Engine::Engine(const pairhmm_options_t& opts) : opts_(opts) {
+    rules_ = opts_.mode == PAIRHMM_MODE_PLAIN ? plain_rules() : engine_default_rules();
+}
+
+Engine::~Engine() {
+    if (ready_) cudaSetDevice(opts_.device);
+    if (graph_exec_) cudaGraphExecDestroy(graph_exec_);
+    DevBuf* bufs[] = {&ph2pr_, &rules_maxlen_, &rules_rank_, &per_task_, &config_, &in_read_bases_, &in_bq_,
+                      &in_iq_, &in_dq_, &in_read_off_, &in_read_len_, &in_hap_bases_, &in_hap_off_, &in_hap_len_,
+                      &read_record_, &read_local_, &rec_haps_, &rec_hap_base_, &rec_pair_base_, &read_start_,
+                      &hap_start_, &read_pack_, &hap_code_, &hist_, &cursor_, &items_, &rescue_, &counters_,
+                      &sched_, &scores_, &scratch_, &lens_tmp_};
+    for (DevBuf* b : bufs) b->release();
+    if (pinned_) cudaFreeHost(pinned_);
+    if (ev0_) cudaEventDestroy(ev0_);
+    if (ev1_) cudaEventDestroy(ev1_);
+    if (ev_prep_) cudaEventDestroy(ev_prep_);
+    if (ev_fp32_) cudaEventDestroy(ev_fp32_);
+    if (stream_) cudaStreamDestroy(stream_);
+}
+
+pairhmm_status_t Engine::fail(pairhmm_status_t s, const std::string& msg) {
+    last_error_ = msg;
+    return s;
+}
+
+pairhmm_status_t Engine::cuda_fail(cudaError_t e, const char* what) {
+    last_error_ = std::string(what) + ": " + cudaGetErrorString(e);
+    return e == cudaErrorMemoryAllocation ? PAIRHMM_ERR_OUT_OF_MEMORY : PAIRHMM_ERR_CUDA;
+}
+
+#define PHMM_CUDA(call)                                   \
+    do {                                                  \
+        cudaError_t e_ = (call);                          \
+        if (e_ != cudaSuccess) return cuda_fail(e_, #call); \
+    } while (0)
+
+pairhmm_status_t Engine::init() {
+    int ndev = 0;
+    cudaError_t e = cudaGetDeviceCount(&ndev);
+    if (e != cudaSuccess || ndev == 0) return fail(PAIRHMM_ERR_UNSUPPORTED, "no CUDA device");
+    if (opts_.device < 0 || opts_.device >= ndev) return fail(PAIRHMM_ERR_INVALID_ARGUMENT, "bad device ordinal");
+    PHMM_CUDA(cudaSetDevice(opts_.device));
+    cudaDeviceProp prop{};
+    PHMM_CUDA(cudaGetDeviceProperties(&prop, opts_.device));
+    if (prop.major < 10) return fail(PAIRHMM_ERR_UNSUPPORTED, "the kernels are built for sm_100a");
+    num_sms_ = prop.multiProcessorCount;
+    PHMM_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+    PHMM_CUDA(cudaEventCreate(&ev0_));
+    PHMM_CUDA(cudaEventCreate(&ev1_));
+    PHMM_CUDA(cudaEventCreate(&ev_prep_));
+    PHMM_CUDA(cudaEventCreate(&ev_fp32_));
+
+    // dynamic shared memory opt-in for every kernel on this device
+    for (const ConfigInfo& c : fp32_configs())
+        PHMM_CUDA(cudaFuncSetAttribute(c.kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c.smem_bytes));
+    PHMM_CUDA(cudaFuncSetAttribute(fp64_kernel(), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)fp64_smem_bytes()));
+
+    // probability table p(q) = float(10^(-q/10)) (gpuworker.cuh:473-486)
+    float table[128];
+    for (int i = 0; i < 128; ++i) table[i] = (float)std::pow(10.0, (-i) / 10.0);
+    PHMM_CUDA(ph2pr_.ensure(sizeof(table)));
+    PHMM_CUDA(cudaMemcpy(ph2pr_.ptr, table, sizeof(table), cudaMemcpyHostToDevice));
+    PHMM_CUDA(counters_.ensure(sizeof(unsigned long long) * (kMaxBuckets + 4)));
+    PHMM_CUDA(sched_.ensure(sizeof(Schedule)));
+    ready_ = true;
+    return upload_rules();
+}
+
+pairhmm_status_t Engine::set_tile_table(const std::vector<TileRule>& rules) {
+    if (rules.empty() || (int)rules.size() > kMaxBuckets) return fail(PAIRHMM_ERR_INVALID_ARGUMENT, "tile table size");
+    for (size_t i = 0; i < rules.size(); ++i) {
+        if (!find_fp32_config(rules[i].G, rules[i].R, rules[i].multi_tile))
+            return fail(PAIRHMM_ERR_INVALID_ARGUMENT, "tile table names a configuration that is not compiled");
+        if (i > 0 && rules[i].max_len <= rules[i - 1].max_len)
+            return fail(PAIRHMM_ERR_INVALID_ARGUMENT, "tile table bounds must increase");
+        if (!rules[i].multi_tile && rules[i].max_len > rules[i].G * rules[i].R)
+            return fail(PAIRHMM_ERR_INVALID_ARGUMENT, "single-tile rule shorter than its bucket");
+    }
+    if (!rules.back().multi_tile) return fail(PAIRHMM_ERR_INVALID_ARGUMENT, "last rule must be multi-tile");
+    rules_ = rules;
+    if (graph_exec_) {
+        cudaGraphExecDestroy(graph_exec_);
+        graph_exec_ = nullptr;
+    }
+    return ready_ ? upload_rules() : PAIRHMM_OK;
+}
+
+pairhmm_status_t Engine::upload_rules() {
+    const int nb = (int)rules_.size();
+    rule_cfg_.assign(nb, nullptr);
+    std::vector<int32_t> maxlen(nb), rank(nb), per(nb), cfg(nb);
+    for (int b = 0; b < nb; ++b) {
+        rule_cfg_[b] = find_fp32_config(rules_[b].G, rules_[b].R, rules_[b].multi_tile);
+        if (!rule_cfg_[b]) return fail(PAIRHMM_ERR_INVALID_ARGUMENT, "tile rule without compiled kernel");
+        maxlen[b] = rules_[b].max_len;
+        rank[b] = opts_.mode == PAIRHMM_MODE_PLAIN ? b : nb - 1 - b;
+    }
+    for (int b = 0; b < nb; ++b) {
+        per[rank[b]] = rule_cfg_[b]->per_warp();
+        cfg[rank[b]] = b;
+    }
+    PHMM_CUDA(rules_maxlen_.ensure(sizeof(int32_t) * nb));
+    PHMM_CUDA(rules_rank_.ensure(sizeof(int32_t) * nb));
+    PHMM_CUDA(per_task_.ensure(sizeof(int32_t) * nb));
+    PHMM_CUDA(config_.ensure(sizeof(int32_t) * nb));
+    PHMM_CUDA(cudaMemcpy(rules_maxlen_.ptr, maxlen.data(), sizeof(int32_t) * nb, cudaMemcpyHostToDevice));
+    PHMM_CUDA(cudaMemcpy(rules_rank_.ptr, rank.data(), sizeof(int32_t) * nb, cudaMemcpyHostToDevice));
+    PHMM_CUDA(cudaMemcpy(per_task_.ptr, per.data(), sizeof(int32_t) * nb, cudaMemcpyHostToDevice));
+    PHMM_CUDA(cudaMemcpy(config_.ptr, cfg.data(), sizeof(int32_t) * nb, cudaMemcpyHostToDevice));
+    return PAIRHMM_OK;
+}
+
+pairhmm_status_t Engine::build_index(const pairhmm_batch_t& b, const std::vector<TileRule>& rules, BatchIndex& x,
+                                     std::string& err) {
+    x = BatchIndex{};
+    if (b.num_records < 0) { err = "num_records < 0"; return PAIRHMM_ERR_INVALID_ARGUMENT; }
+    x.num_records = b.num_records;
+    if (b.num_records == 0) return PAIRHMM_OK;
+    if (!b.reads_per_record || !b.haps_per_record) { err = "null record arrays"; return PAIRHMM_ERR_INVALID_ARGUMENT; }
+    x.rec_haps.resize(b.num_records);
+    x.rec_hap_base.resize(b.num_records);
+    x.rec_pair_base.resize(b.num_records);
+    for (int64_t g = 0; g < b.num_records; ++g) {
+        const int32_t R = b.reads_per_record[g], H = b.haps_per_record[g];
+        if (R < 0 || H < 0) { err = "negative reads/haplotypes in a record"; return PAIRHMM_ERR_INVALID_ARGUMENT; }
+        x.rec_haps[g] = H;
+        x.rec_hap_base[g] = x.num_haps;
+        x.rec_pair_base[g] = x.num_pairs;
+        x.num_reads += R;
+        x.num_haps += H;
+        x.num_pairs += (int64_t)R * H;
+    }
+    if (x.num_reads >= (int64_t(1) << 31) || x.num_haps >= (int64_t(1) << 31)) {
+        err = "more than 2^31-1 reads or haplotypes in one batch";
+        return PAIRHMM_ERR_INVALID_ARGUMENT;
+    }
+    if ((x.num_reads && (!b.read_lengths)) || (x.num_haps && !b.hap_lengths)) {
+        err = "null length arrays";
+        return PAIRHMM_ERR_INVALID_ARGUMENT;
+    }
+    x.read_record.resize(x.num_reads);
+    x.read_local.resize(x.num_reads);
+    x.read_start.resize(x.num_reads);
+    x.hap_start.resize(x.num_haps);
+    x.bucket_pairs.assign(rules.size(), 0);
+    {
+        int64_t i = 0;
+        for (int64_t g = 0; g < b.num_records; ++g)
+            for (int32_t r = 0; r < b.reads_per_record[g]; ++r, ++i) {
+                x.read_record[i] = (int32_t)g;
+                x.read_local[i] = r;
+            }
+    }
+    for (int64_t i = 0; i < x.num_reads; ++i) {
+        const int32_t L = b.read_lengths[i];
+        if (L < 1) { err = "read length < 1"; return PAIRHMM_ERR_INVALID_ARGUMENT; }
+        if (b.read_offsets) {
+            if (b.read_offsets[i] < 0) { err = "negative read offset"; return PAIRHMM_ERR_INVALID_ARGUMENT; }
+            x.read_bytes = std::max<int64_t>(x.read_bytes, b.read_offsets[i] + L);
+            x.read_min = i == 0 ? b.read_offsets[i] : std::min<int64_t>(x.read_min, b.read_offsets[i]);
+        }
+        x.max_read_len = std::max(x.max_read_len, L);
+        x.read_start[i] = x.pack_positions;
+        x.pack_positions += round_up(L, 4);
+        const int bk = bucket_of_host(L, rules);
+        const int64_t H = x.rec_haps[x.read_record[i]];
+        x.bucket_pairs[bk] += H;
+        if (rules[bk].multi_tile) x.multi_tile_pairs += H;
+    }
+    for (int64_t h = 0; h < x.num_haps; ++h) {
+        const int32_t H = b.hap_lengths[h];
+        if (H < 1) { err = "haplotype length < 1"; return PAIRHMM_ERR_INVALID_ARGUMENT; }
+        if (b.hap_offsets) {
+            if (b.hap_offsets[h] < 0) { err = "negative haplotype offset"; return PAIRHMM_ERR_INVALID_ARGUMENT; }
+            x.hap_bytes = std::max<int64_t>(x.hap_bytes, b.hap_offsets[h] + H);
+            x.hap_min = h == 0 ? b.hap_offsets[h] : std::min<int64_t>(x.hap_min, b.hap_offsets[h]);
+        }
+        x.max_hap_len = std::max(x.max_hap_len, H);
+        x.hap_start[h] = x.code_bytes;
+        x.code_bytes += round_up(H, 16);
+    }
+    // cells: sum over records of (sum L) * (sum H)  (gpuworker.cuh:495-520)
+    {
+        int64_t i = 0;
+        for (int64_t g = 0; g < b.num_records; ++g) {
+            int64_t sl = 0, sh = 0;
+            for (int32_t r = 0; r < b.reads_per_record[g]; ++r, ++i) sl += b.read_lengths[i];
+            for (int32_t h = 0; h < b.haps_per_record[g]; ++h) sh += b.hap_lengths[x.rec_hap_base[g] + h];
+            x.cells += sl * sh;
+        }
+    }
+    return PAIRHMM_OK;
+}
+
+pairhmm_status_t Engine::ensure_buffers(const BatchIndex& x, bool host_inputs) {
+    const int64_t nr = std::max<int64_t>(x.num_reads, 1), nh = std::max<int64_t>(x.num_haps, 1);
+    const int64_t ng = std::max<int64_t>(x.num_records, 1), np = std::max<int64_t>(x.num_pairs, 1);
+    if (host_inputs) {
+        const int64_t rb = std::max<int64_t>(x.read_bytes - x.read_min, 1);
+        const int64_t hb = std::max<int64_t>(x.hap_bytes - x.hap_min, 1);
+        PHMM_CUDA(in_read_bases_.ensure(rb));
+        PHMM_CUDA(in_bq_.ensure(rb));
+        PHMM_CUDA(in_iq_.ensure(rb));
+        PHMM_CUDA(in_dq_.ensure(rb));
+        PHMM_CUDA(in_read_off_.ensure(8 * nr));
+        PHMM_CUDA(in_read_len_.ensure(4 * nr));
+        PHMM_CUDA(in_hap_bases_.ensure(hb));
+        PHMM_CUDA(in_hap_off_.ensure(8 * nh));
+        PHMM_CUDA(in_hap_len_.ensure(4 * nh));
+        PHMM_CUDA(scores_.ensure(4 * np));
+    }
+    PHMM_CUDA(read_record_.ensure(4 * nr));
+    PHMM_CUDA(read_local_.ensure(4 * nr));
+    PHMM_CUDA(rec_haps_.ensure(4 * ng));
+    PHMM_CUDA(rec_hap_base_.ensure(8 * ng));
+    PHMM_CUDA(rec_pair_base_.ensure(8 * ng));
+    PHMM_CUDA(read_start_.ensure(8 * nr));
+    PHMM_CUDA(hap_start_.ensure(8 * nh));
+    PHMM_CUDA(read_pack_.ensure(4 * (x.pack_positions + kReadSlackPos)));
+    PHMM_CUDA(hap_code_.ensure(x.code_bytes + kHapSlack));
+    const int64_t nbins = (int64_t)rules_.size() * (opts_.mode == PAIRHMM_MODE_PLAIN ? 1 : kHBins);
+    PHMM_CUDA(hist_.ensure(4 * nbins));
+    PHMM_CUDA(cursor_.ensure(8 * nbins));
+    PHMM_CUDA(items_.ensure(sizeof(Task) * np));
+    PHMM_CUDA(rescue_.ensure(sizeof(Task) * np));
+    return PAIRHMM_OK;
+}
+
+pairhmm_status_t Engine::upload_index(const BatchIndex& x, cudaStream_t s) {
+    struct Piece { DevBuf* dst; const void* src; size_t bytes; };
+    const Piece pieces[] = {
+        {&read_record_, x.read_record.data(), 4 * x.read_record.size()},
+        {&read_local_, x.read_local.data(), 4 * x.read_local.size()},
+        {&rec_haps_, x.rec_haps.data(), 4 * x.rec_haps.size()},
+        {&rec_hap_base_, x.rec_hap_base.data(), 8 * x.rec_hap_base.size()},
+        {&rec_pair_base_, x.rec_pair_base.data(), 8 * x.rec_pair_base.size()},
+        {&read_start_, x.read_start.data(), 8 * x.read_start.size()},
+        {&hap_start_, x.hap_start.data(), 8 * x.hap_start.size()},
+    };
+    size_t total = 0;
+    for (const Piece& p : pieces) total += round_up((int64_t)p.bytes, 256);
+    if (total > pinned_cap_) {
+        PHMM_CUDA(cudaStreamSynchronize(s));
+        if (pinned_) cudaFreeHost(pinned_);
+        pinned_ = nullptr;
+        pinned_cap_ = 0;
+        PHMM_CUDA(cudaMallocHost(&pinned_, total + total / 4));
+        pinned_cap_ = total + total / 4;
+    } else {
+        // the previous upload may still be in flight
+        PHMM_CUDA(cudaStreamSynchronize(s));
+    }
+    size_t off = 0;
+    for (const Piece& p : pieces) {
+        if (p.bytes == 0) continue;
+        char* dst = static_cast<char*>(pinned_) + off;
+        std::memcpy(dst, p.src, p.bytes);
+        PHMM_CUDA(cudaMemcpyAsync(p.dst->ptr, dst, p.bytes, cudaMemcpyHostToDevice, s));
+        off += round_up((int64_t)p.bytes, 256);
+    }
+    return PAIRHMM_OK;
+}
+
+int64_t Engine::index_bytes(const BatchIndex& x) {
+    return 4 * (int64_t)(x.read_record.size() + x.read_local.size() + x.rec_haps.size()) +
+           8 * (int64_t)(x.rec_hap_base.size() + x.rec_pair_base.size() + x.read_start.size() + x.hap_start.size());
+}
+
+int Engine::persistent_grid(const void* kernel, size_t smem) const {
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kBlockThreads, smem) != cudaSuccess ||
+        per_sm < 1)
+        per_sm = 1;
+    return per_sm * num_sms_;
+}
+
+pairhmm_status_t Engine::enqueue_pipeline(const pairhmm_batch_t& in, const BatchIndex& x, const Plan& plan,
+                                          float* d_scores, cudaStream_t s) {
+    const int nb = (int)rules_.size();
+    const bool plain = opts_.mode == PAIRHMM_MODE_PLAIN;
+    const int prep_grid = 4 * num_sms_;
+
+    PrepArgs pa{};
+    pa.read_bases = in.read_bases;
+    pa.base_quals = in.base_quals;
+    pa.ins_quals = in.ins_quals;
+    pa.del_quals = in.del_quals;
+    pa.read_offsets = in.read_offsets;
+    pa.read_lengths = in.read_lengths;
+    pa.hap_bases = in.hap_bases;
+    pa.hap_offsets = in.hap_offsets;
+    pa.hap_lengths = in.hap_lengths;
+    pa.read_record = read_record_.as<int32_t>();
+    pa.read_local = read_local_.as<int32_t>();
+    pa.rec_haps = rec_haps_.as<int32_t>();
+    pa.rec_hap_base = rec_hap_base_.as<int64_t>();
+    pa.rec_pair_base = rec_pair_base_.as<int64_t>();
+    pa.read_start = read_start_.as<int64_t>();
+    pa.hap_start = hap_start_.as<int64_t>();
+    pa.num_reads = x.num_reads;
+    pa.num_haps = x.num_haps;
+    pa.read_pack = read_pack_.as<uint32_t>();
+    pa.hap_code = hap_code_.as<uint8_t>();
+    launches_ = 0;
+    PHMM_CUDA(launch_pack(pa, prep_grid, s));
+    launches_ += 2;
+    PHMM_CUDA(cudaMemsetAsync(hap_code_.as<uint8_t>() + x.code_bytes, 4, kHapSlack, s));
+
+    BinArgs ba{};
+    ba.read_lengths = in.read_lengths;
+    ba.hap_lengths = in.hap_lengths;
+    ba.read_record = pa.read_record;
+    ba.read_local = pa.read_local;
+    ba.rec_haps = pa.rec_haps;
+    ba.rec_hap_base = pa.rec_hap_base;
+    ba.rec_pair_base = pa.rec_pair_base;
+    ba.num_reads = x.num_reads;
+    ba.nbuckets = nb;
+    ba.hbins = plain ? 1 : kHBins;
+    ba.bucket_max_len = rules_maxlen_.as<int32_t>();
+    ba.bucket_rank = rules_rank_.as<int32_t>();
+    ba.hist = hist_.as<unsigned int>();
+    ba.cursor = cursor_.as<unsigned long long>();
+    ba.items = items_.as<Task>();
+    PHMM_CUDA(launch_binning(ba, prep_grid, s, per_task_.as<int>(), config_.as<int>(), sched_.as<Schedule>(), nb));
+    launches_ += 4;
+    PHMM_CUDA(cudaMemsetAsync(counters_.ptr, 0, sizeof(unsigned long long) * (kMaxBuckets + 4), s));
+    PHMM_CUDA(cudaEventRecord(ev_prep_, s));
+
+    unsigned long long* counters = counters_.as<unsigned long long>();
+    DevView v{};
+    v.read_pack = pa.read_pack;
+    v.read_start = pa.read_start;
+    v.read_len = in.read_lengths;
+    v.hap_code = pa.hap_code;
+    v.hap_start = pa.hap_start;
+    v.hap_len = in.hap_lengths;
+    v.scores = d_scores;
+    v.rescue = rescue_.as<Task>();
+    v.rescue_count = counters + kMaxBuckets;
+    v.rescue_enabled = (!plain && opts_.fp64_rescue) ? 1 : 0;
+    v.ph2pr = ph2pr_.as<float>();
+
+    for (int rank = 0; rank < nb; ++rank) {
+        const int b = plain ? rank : nb - 1 - rank;
+        if (x.bucket_pairs[b] == 0) continue;
+        const ConfigInfo* c = rule_cfg_[b];
+        Fp32LaunchArgs la{};
+        la.view = v;
+        la.items = items_.as<Task>();
+        la.sched = sched_.as<Schedule>();
+        la.rank = rank;
+        la.persistent = plan.persistent[b];
+        la.counter = counters + rank;
+        la.scratch = scratch_.ptr;
+        la.rows = plan.rows;
+        la.grid = plan.grid[b];
+        la.stream = s;
+        PHMM_CUDA(c->launch(la));
+        ++launches_;
+    }
+    PHMM_CUDA(cudaEventRecord(ev_fp32_, s));
+    // FP64 pass over flagged pairs (FP32 underflow, or degenerate alpha)
+    {
+        Fp64LaunchArgs fa{};
+        fa.view = v;
+        fa.items = rescue_.as<Task>();
+        fa.count = counters + kMaxBuckets;
+        fa.counter = counters + kMaxBuckets + 1;
+        fa.scratch = scratch_.ptr;
+        fa.rows = plan.rows;
+        fa.grid = plan.fp64_grid;
+        fa.stream = s;
+        PHMM_CUDA(launch_fp64_rescue(fa));
+        ++launches_;
+    }
+    return PAIRHMM_OK;
+}
+
+Engine::Plan Engine::make_plan(const BatchIndex& x) const {
+    const int nb = (int)rules_.size();
+    const bool plain = opts_.mode == PAIRHMM_MODE_PLAIN;
+    Plan p;
+    p.rows = round_up((int64_t)x.max_hap_len + 2 * 32 + 8, 64);
+    p.grid.assign(nb, 0);
+    p.persistent.assign(nb, 1);
+    int64_t scratch = 0;
+    for (int b = 0; b < nb; ++b) {
+        if (x.bucket_pairs[b] == 0) continue;
+        const ConfigInfo* c = rule_cfg_[b];
+        const int64_t tasks = (x.bucket_pairs[b] + c->per_warp() - 1) / c->per_warp();
+        const int64_t need_blocks = (tasks + kWarpsPerBlock - 1) / kWarpsPerBlock;
+        int64_t grid = plain ? need_blocks : std::min<int64_t>(persistent_grid(c->kernel, c->smem_bytes), need_blocks);
+        if (c->multi_tile) {
+            const int64_t per_warp = (int64_t)c->scratch_bytes_per_row * p.rows;
+            const int64_t cap_blocks = std::max<int64_t>(1, kScratchBudget / (per_warp * kWarpsPerBlock));
+            grid = std::min(grid, cap_blocks);
+            scratch = std::max(scratch, grid * kWarpsPerBlock * per_warp);
+        }
+        grid = std::max<int64_t>(1, std::min<int64_t>(grid, INT32_MAX));
+        p.grid[b] = (int)grid;
+        // the plain form runs one task per warp; a grid capped by scratch loops on the counter
+        p.persistent[b] = (!plain || grid < need_blocks) ? 1 : 0;
+    }
+    {
+        const int64_t per_warp = (int64_t)fp64_scratch_bytes_per_row() * p.rows;
+        int64_t grid = persistent_grid(fp64_kernel(), fp64_smem_bytes());
+        grid = std::min<int64_t>(grid, std::max<int64_t>(1, kScratchBudget / (per_warp * kWarpsPerBlock)));
+        p.fp64_grid = (int)grid;
+        scratch = std::max(scratch, grid * kWarpsPerBlock * per_warp);
+    }
+    p.scratch_bytes = (size_t)std::max<int64_t>(scratch, 256);
+    return p;
+}
+
+pairhmm_status_t Engine::run_pipeline(const pairhmm_batch_t& in, const BatchIndex& x, float* d_scores,
+                                      cudaStream_t s) {
+    if (x.num_pairs == 0) return PAIRHMM_OK;
+    // every buffer the launches reference exists before capture starts
+    const Plan plan = make_plan(x);
+    PHMM_CUDA(scratch_.ensure(plan.scratch_bytes));
+    if (!opts_.use_graphs) return enqueue_pipeline(in, x, plan, d_scores, s);
+
+    cudaGraph_t graph = nullptr;
+    PHMM_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    pairhmm_status_t st = enqueue_pipeline(in, x, plan, d_scores, s);
+    cudaError_t ce = cudaStreamEndCapture(s, &graph);
+    if (st != PAIRHMM_OK) {
+        if (graph) cudaGraphDestroy(graph);
+        return st;
+    }
+    if (ce != cudaSuccess) return cuda_fail(ce, "cudaStreamEndCapture");
+    bool updated = false;
+    if (graph_exec_) {
+        cudaGraphExecUpdateResultInfo info{};
+        if (cudaGraphExecUpdate(graph_exec_, graph, &info) == cudaSuccess) updated = true;
+        else {
+            cudaGetLastError();
+            cudaGraphExecDestroy(graph_exec_);
+            graph_exec_ = nullptr;
+        }
+    }
+    if (!updated) {
+        ce = cudaGraphInstantiate(&graph_exec_, graph, 0);
+        if (ce != cudaSuccess) {
+            cudaGraphDestroy(graph);
+            graph_exec_ = nullptr;
+            return cuda_fail(ce, "cudaGraphInstantiate");
+        }
+    }
+    cudaGraphDestroy(graph);
+    PHMM_CUDA(cudaGraphLaunch(graph_exec_, s));
+    return PAIRHMM_OK;
+}
+
+pairhmm_status_t Engine::compute_host(const pairhmm_batch_t& b, float* scores) {
+    const auto t0 = std::chrono::steady_clock::now();
+    PHMM_CUDA(cudaSetDevice(opts_.device));
+    BatchIndex x;
+    std::string err;
+    pairhmm_status_t st = build_index(b, rules_, x, err);
+    if (st != PAIRHMM_OK) return fail(st, err);
+    if (x.num_pairs > 0 && !scores) return fail(PAIRHMM_ERR_INVALID_ARGUMENT, "null scores");
+    if (x.num_reads > 0 && (!b.read_bases || !b.base_quals || !b.ins_quals || !b.del_quals || !b.read_offsets))
+        return fail(PAIRHMM_ERR_INVALID_ARGUMENT, "null read arrays");
+    if (x.num_haps > 0 && (!b.hap_bases || !b.hap_offsets)) return fail(PAIRHMM_ERR_INVALID_ARGUMENT, "null haplotype arrays");
+    stats_ = pairhmm_stats_t{};
+    stats_.pairs = x.num_pairs;
+    stats_.cells = x.cells;
+    stats_.multi_tile_pairs = x.multi_tile_pairs;
+    if (x.num_pairs == 0) return PAIRHMM_OK;
+    if ((st = ensure_buffers(x, true)) != PAIRHMM_OK) return st;
+    cudaStream_t s = stream_;
+    // only the byte range the batch references is copied; device base pointers
+    // are shifted so the caller's absolute offsets stay valid
+    const int64_t rlo = x.read_min, rn = x.read_bytes - x.read_min;
+    const int64_t hlo = x.hap_min, hn = x.hap_bytes - x.hap_min;
+    PHMM_CUDA(cudaMemcpyAsync(in_read_bases_.ptr, b.read_bases + rlo, rn, cudaMemcpyHostToDevice, s));
+    PHMM_CUDA(cudaMemcpyAsync(in_bq_.ptr, b.base_quals + rlo, rn, cudaMemcpyHostToDevice, s));
+    PHMM_CUDA(cudaMemcpyAsync(in_iq_.ptr, b.ins_quals + rlo, rn, cudaMemcpyHostToDevice, s));
+    PHMM_CUDA(cudaMemcpyAsync(in_dq_.ptr, b.del_quals + rlo, rn, cudaMemcpyHostToDevice, s));
+    PHMM_CUDA(cudaMemcpyAsync(in_read_off_.ptr, b.read_offsets, 8 * x.num_reads, cudaMemcpyHostToDevice, s));
+    PHMM_CUDA(cudaMemcpyAsync(in_read_len_.ptr, b.read_lengths, 4 * x.num_reads, cudaMemcpyHostToDevice, s));
+    PHMM_CUDA(cudaMemcpyAsync(in_hap_bases_.ptr, b.hap_bases + hlo, hn, cudaMemcpyHostToDevice, s));
+    PHMM_CUDA(cudaMemcpyAsync(in_hap_off_.ptr, b.hap_offsets, 8 * x.num_haps, cudaMemcpyHostToDevice, s));
+    PHMM_CUDA(cudaMemcpyAsync(in_hap_len_.ptr, b.hap_lengths, 4 * x.num_haps, cudaMemcpyHostToDevice, s));
+    if ((st = upload_index(x, s)) != PAIRHMM_OK) return st;
+
+    pairhmm_batch_t dev = b;
+    auto shifted = [](const DevBuf& d, int64_t lo) {
+        return reinterpret_cast<const uint8_t*>(reinterpret_cast<uintptr_t>(d.ptr) - (uintptr_t)lo);
+    };
+    dev.read_bases = shifted(in_read_bases_, rlo);
+    dev.base_quals = shifted(in_bq_, rlo);
+    dev.ins_quals = shifted(in_iq_, rlo);
+    dev.del_quals = shifted(in_dq_, rlo);
+    dev.gcp_quals = nullptr;
+    dev.read_offsets = in_read_off_.as<int64_t>();
+    dev.read_lengths = in_read_len_.as<int32_t>();
+    dev.hap_bases = shifted(in_hap_bases_, hlo);
+    dev.hap_offsets = in_hap_off_.as<int64_t>();
+    dev.hap_lengths = in_hap_len_.as<int32_t>();
+
+    PHMM_CUDA(cudaEventRecord(ev0_, s));
+    if ((st = run_pipeline(dev, x, scores_.as<float>(), s)) != PAIRHMM_OK) return st;
+    PHMM_CUDA(cudaEventRecord(ev1_, s));
+    PHMM_CUDA(cudaMemcpyAsync(scores, scores_.ptr, 4 * x.num_pairs, cudaMemcpyDeviceToHost, s));
+    unsigned long long rescued = 0;
+    PHMM_CUDA(cudaMemcpyAsync(&rescued, counters_.as<unsigned long long>() + kMaxBuckets, sizeof(rescued),
+                              cudaMemcpyDeviceToHost, s));
+    PHMM_CUDA(cudaStreamSynchronize(s));
+    float ms = 0.f, a = 0.f, b2 = 0.f, c = 0.f;
+    PHMM_CUDA(cudaEventElapsedTime(&ms, ev0_, ev1_));
+    PHMM_CUDA(cudaEventElapsedTime(&a, ev0_, ev_prep_));
+    PHMM_CUDA(cudaEventElapsedTime(&b2, ev_prep_, ev_fp32_));
+    PHMM_CUDA(cudaEventElapsedTime(&c, ev_fp32_, ev1_));
+    stats_.device_ms = ms;
+    stats_.prep_ms = a;
+    stats_.fp32_ms = b2;
+    stats_.fp64_ms = c;
+    stats_.launches = launches_;
+    stats_.h2d_bytes = 4 * rn + hn + 12 * x.num_reads + 12 * x.num_haps + index_bytes(x);
+    stats_.d2h_bytes = 4 * x.num_pairs + (int64_t)sizeof(rescued);
+    stats_.rescued = (int64_t)rescued;
+    stats_.total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    return PAIRHMM_OK;
+}
+
+pairhmm_status_t Engine::compute_device(const pairhmm_batch_t& b, int32_t, int32_t, float* scores,
+                                        cudaStream_t stream) {
+    const auto t0 = std::chrono::steady_clock::now();
+    PHMM_CUDA(cudaSetDevice(opts_.device));
+    if (b.num_records < 0) return fail(PAIRHMM_ERR_INVALID_ARGUMENT, "num_records < 0");
+    if (b.num_records == 0) { stats_ = pairhmm_stats_t{}; return PAIRHMM_OK; }
+    if (!b.reads_per_record || !b.haps_per_record) return fail(PAIRHMM_ERR_INVALID_ARGUMENT, "null record arrays");
+    // the host needs the record structure and lengths to derive the index
+    std::vector<int32_t> rpr(b.num_records), hpr(b.num_records);
+    PHMM_CUDA(cudaMemcpyAsync(rpr.data(), b.reads_per_record, 4 * b.num_records, cudaMemcpyDeviceToHost, stream));
+    PHMM_CUDA(cudaMemcpyAsync(hpr.data(), b.haps_per_record, 4 * b.num_records, cudaMemcpyDeviceToHost, stream));
+    PHMM_CUDA(cudaStreamSynchronize(stream));
+    int64_t nr = 0, nh = 0;
+    for (int64_t g = 0; g < b.num_records; ++g) { nr += std::max(rpr[g], 0); nh += std::max(hpr[g], 0); }
+    std::vector<int32_t> rl(nr), hl(nh);
+    if (nr) PHMM_CUDA(cudaMemcpyAsync(rl.data(), b.read_lengths, 4 * nr, cudaMemcpyDeviceToHost, stream));
+    if (nh) PHMM_CUDA(cudaMemcpyAsync(hl.data(), b.hap_lengths, 4 * nh, cudaMemcpyDeviceToHost, stream));
+    PHMM_CUDA(cudaStreamSynchronize(stream));
+    pairhmm_batch_t hb = b;
+    hb.reads_per_record = rpr.data();
+    hb.haps_per_record = hpr.data();
+    hb.read_lengths = rl.data();
+    hb.hap_lengths = hl.data();
+    hb.read_offsets = nullptr;
+    hb.hap_offsets = nullptr;
+    BatchIndex x;
+    std::string err;
+    pairhmm_status_t st = build_index(hb, rules_, x, err);
+    if (st != PAIRHMM_OK) return fail(st, err);
+    stats_ = pairhmm_stats_t{};
+    stats_.pairs = x.num_pairs;
+    stats_.cells = x.cells;
+    stats_.multi_tile_pairs = x.multi_tile_pairs;
+    stats_.rescued = -1;
+    if (x.num_pairs == 0) return PAIRHMM_OK;
+    if (!scores) return fail(PAIRHMM_ERR_INVALID_ARGUMENT, "null scores");
+    if ((st = ensure_buffers(x, false)) != PAIRHMM_OK) return st;
+    cudaStream_t s = stream_;
+    PHMM_CUDA(cudaEventRecord(ev0_, stream));
+    PHMM_CUDA(cudaStreamWaitEvent(s, ev0_, 0));
+    if ((st = upload_index(x, s)) != PAIRHMM_OK) return st;
+    PHMM_CUDA(cudaEventRecord(ev0_, s));
+    if ((st = run_pipeline(b, x, scores, s)) != PAIRHMM_OK) return st;
+    PHMM_CUDA(cudaEventRecord(ev1_, s));
+    PHMM_CUDA(cudaStreamWaitEvent(stream, ev1_, 0));
+    stats_.total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    stats_.device_ms = -1.0;
+    return PAIRHMM_OK;
+}
+
+}  // namespace phmm

@@ -1,0 +1,115 @@
+// Host-side engine behind the C ABI.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/pairhmm_b200.h"
+#include "kernels.hpp"
+
+namespace phmm {
+
+// One entry of a tile table: reads with length <= max_len (and above the
+// previous entry's bound) run with (G, R, multi_tile).
+struct TileRule {
+    int max_len;
+    int G;
+    int R;
+    bool multi_tile;
+};
+
+// Per-batch index derived on the host from the record structure.
+struct BatchIndex {
+    int64_t num_records = 0, num_reads = 0, num_haps = 0, num_pairs = 0, cells = 0;
+    int32_t max_read_len = 0, max_hap_len = 0;
+    int64_t read_bytes = 0, hap_bytes = 0;          // end of the caller's referenced byte range
+    int64_t read_min = 0, hap_min = 0;              // start of that range
+    int64_t pack_positions = 0, code_bytes = 0;     // packed extents
+    std::vector<int32_t> read_record, read_local, rec_haps;
+    std::vector<int64_t> rec_hap_base, rec_pair_base, read_start, hap_start;
+    std::vector<int64_t> bucket_pairs;              // by bucket index
+    int64_t multi_tile_pairs = 0;
+};
+
+// Grow-only device buffer.
+struct DevBuf {
+    void* ptr = nullptr;
+    size_t cap = 0;
+    cudaError_t ensure(size_t bytes);
+    void release();
+    template <class T> T* as() const { return static_cast<T*>(ptr); }
+};
+
+class Engine {
+public:
+    explicit Engine(const pairhmm_options_t& opts);
+    ~Engine();
+    Engine(const Engine&) = delete;
+    Engine& operator=(const Engine&) = delete;
+
+    pairhmm_status_t init();
+    pairhmm_status_t compute_host(const pairhmm_batch_t& b, float* scores);
+    pairhmm_status_t compute_device(const pairhmm_batch_t& b, int32_t max_read_len, int32_t max_hap_len,
+                                    float* scores, cudaStream_t stream);
+    const pairhmm_stats_t& stats() const { return stats_; }
+    const std::string& last_error() const { return last_error_; }
+    pairhmm_status_t fail(pairhmm_status_t s, const std::string& msg);
+    pairhmm_status_t cuda_fail(cudaError_t e, const char* what);
+
+    // Replace the tile table of the current mode (autotuner).
+    pairhmm_status_t set_tile_table(const std::vector<TileRule>& rules);
+    const std::vector<TileRule>& tile_table() const { return rules_; }
+    int device() const { return opts_.device; }
+    int64_t budget_bytes() const { return opts_.device_budget_bytes; }
+    int num_sms() const { return num_sms_; }
+
+    static pairhmm_status_t build_index(const pairhmm_batch_t& b, const std::vector<TileRule>& rules,
+                                        BatchIndex& idx, std::string& err);
+
+private:
+    pairhmm_status_t upload_rules();
+    pairhmm_status_t run_pipeline(const pairhmm_batch_t& dev_in, const BatchIndex& idx, float* d_scores,
+                                  cudaStream_t s);
+    struct Plan {
+        int64_t rows = 0;                 // border rows per buffer
+        std::vector<int> grid;            // by bucket
+        std::vector<int> persistent;      // by bucket
+        int fp64_grid = 0;
+        size_t scratch_bytes = 0;
+    };
+    Plan make_plan(const BatchIndex& idx) const;
+    pairhmm_status_t enqueue_pipeline(const pairhmm_batch_t& dev_in, const BatchIndex& idx, const Plan& plan,
+                                      float* d_scores, cudaStream_t s);
+    pairhmm_status_t ensure_buffers(const BatchIndex& idx, bool host_inputs);
+    pairhmm_status_t upload_index(const BatchIndex& idx, cudaStream_t s);
+    int persistent_grid(const void* kernel, size_t smem) const;
+    static int64_t index_bytes(const BatchIndex& x);
+
+    pairhmm_options_t opts_;
+    std::vector<TileRule> rules_;
+    std::vector<const ConfigInfo*> rule_cfg_;
+    int num_sms_ = 0;
+    bool ready_ = false;
+    cudaStream_t stream_ = nullptr;
+    cudaEvent_t ev0_ = nullptr, ev1_ = nullptr, ev_prep_ = nullptr, ev_fp32_ = nullptr;
+    int64_t launches_ = 0;
+    cudaGraphExec_t graph_exec_ = nullptr;
+    pairhmm_stats_t stats_{};
+    std::string last_error_;
+
+    // device buffers
+    DevBuf ph2pr_, rules_maxlen_, rules_rank_, per_task_, config_;
+    DevBuf in_read_bases_, in_bq_, in_iq_, in_dq_, in_read_off_, in_read_len_;
+    DevBuf in_hap_bases_, in_hap_off_, in_hap_len_;
+    DevBuf read_record_, read_local_, rec_haps_, rec_hap_base_, rec_pair_base_, read_start_, hap_start_;
+    DevBuf read_pack_, hap_code_, hist_, cursor_, items_, rescue_, counters_, sched_, scores_, scratch_;
+    DevBuf lens_tmp_;
+    // pinned staging for the index upload
+    void* pinned_ = nullptr;
+    size_t pinned_cap_ = 0;
+};
+
+}  // namespace phmm

@@ -1,0 +1,72 @@
+// __global__ wrapper around Fp32Wavefront and its registration.
+#pragma once
+
+#include "kernels.hpp"
+#include "wavefront_fp32.cuh"
+
+namespace phmm {
+
+// One kernel per configuration.  persistent = 1: every warp repeatedly takes
+// the next warp task of its bucket from an atomic counter (items are sorted
+// longest first, so this is longest-processing-time-first scheduling).
+// persistent = 0: warp w of the grid runs task w once (one launch per
+// partition, the reference's execution form).
+template <int G, int R, bool MT>
+__global__ void __launch_bounds__(kBlockThreads)
+fp32_bucket_kernel(DevView v, const Task* __restrict__ items, const Schedule* __restrict__ s, int rank,
+                   int persistent, unsigned long long* counter, float4* scratch, int64_t rows) {
+    using W = Fp32Wavefront<G, R, MT>;
+    extern __shared__ float4 smem[];
+    float* ph = reinterpret_cast<float*>(smem);
+    const int warp = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31;
+    float4* wtab = smem + 32 + warp * W::kTableFloat4;
+    for (int i = threadIdx.x; i < 128; i += blockDim.x) ph[i] = v.ph2pr[i];
+    __syncthreads();
+
+    const long long ib = s->item_begin[rank];
+    const long long ie = s->item_begin[rank + 1];
+    const int per = W::NG;
+    const long long ntasks = (ie - ib + per - 1) / per;
+    const long long gwarp = (long long)blockIdx.x * kWarpsPerBlock + warp;
+    float4* wscratch = MT ? scratch + gwarp * (long long)per * 2 * rows : nullptr;
+
+    long long tsk = gwarp;
+    while (true) {
+        if (persistent) {
+            unsigned long long x = 0;
+            if (lane == 0) x = atomicAdd(counter, 1ull);
+            tsk = (long long)__shfl_sync(kFullMask, x, 0);
+        }
+        if (tsk >= ntasks) break;
+        const long long first = ib + tsk * per;
+        const int n = (int)((ie - first) < per ? (ie - first) : per);
+        W::run(v, items + first, n, wtab, ph, wscratch, rows);
+        if (!persistent) break;
+    }
+}
+
+template <int G, int R, bool MT>
+cudaError_t launch_fp32_bucket(const Fp32LaunchArgs& a) {
+    using W = Fp32Wavefront<G, R, MT>;
+    const size_t smem = (32 + (size_t)kWarpsPerBlock * W::kTableFloat4) * sizeof(float4);
+    fp32_bucket_kernel<G, R, MT><<<a.grid, kBlockThreads, smem, a.stream>>>(
+        a.view, a.items, a.sched, a.rank, a.persistent, a.counter, static_cast<float4*>(a.scratch), a.rows);
+    return cudaGetLastError();
+}
+
+template <int G, int R, bool MT>
+ConfigInfo make_fp32_config() {
+    using W = Fp32Wavefront<G, R, MT>;
+    ConfigInfo c{};
+    c.G = G;
+    c.R = R;
+    c.multi_tile = MT;
+    c.smem_bytes = (32 + (size_t)kWarpsPerBlock * W::kTableFloat4) * sizeof(float4);
+    c.scratch_bytes_per_row = MT ? (size_t)W::NG * 2 * sizeof(float4) : 0;
+    c.kernel = reinterpret_cast<const void*>(&fp32_bucket_kernel<G, R, MT>);
+    c.launch = &launch_fp32_bucket<G, R, MT>;
+    return c;
+}
+
+}  // namespace phmm

@@ -1,0 +1,74 @@
+// Host-visible registry of the compiled kernel configurations.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <cstdint>
+#include <vector>
+
+#include "device_common.cuh"
+#include "prep_kernels.cuh"
+
+namespace phmm {
+
+constexpr int kBlockThreads = 128;  // 4 warps per CTA
+constexpr int kWarpsPerBlock = kBlockThreads / 32;
+
+struct Fp32LaunchArgs {
+    DevView view;
+    const Task* items;
+    const Schedule* sched;
+    int rank;                       // bucket rank this launch serves
+    int persistent;                 // 1: warps loop on an atomic task counter
+    unsigned long long* counter;    // per-rank task counter (persistent)
+    void* scratch;                  // multi-tile border storage
+    int64_t rows;                   // border rows per buffer
+    int grid;
+    cudaStream_t stream;
+};
+
+struct Fp64LaunchArgs {
+    DevView view;
+    const Task* items;               // rescue list
+    const unsigned long long* count; // number of items (device)
+    unsigned long long* counter;     // task counter
+    void* scratch;
+    int64_t rows;
+    int grid;
+    cudaStream_t stream;
+};
+
+struct ConfigInfo {
+    int G;
+    int R;
+    bool multi_tile;
+    int tile() const { return G * R; }
+    int per_warp() const { return 32 / G; }
+    size_t smem_bytes;               // dynamic shared memory per CTA
+    size_t scratch_bytes_per_row;    // per warp, per border row (both buffers)
+    const void* kernel;
+    cudaError_t (*launch)(const Fp32LaunchArgs&);
+};
+
+// All compiled FP32 configurations.
+const std::vector<ConfigInfo>& fp32_configs();
+const ConfigInfo* find_fp32_config(int G, int R, bool multi_tile);
+
+// FP64 rescue kernel (G = 32, R = 8, multi-tile capable).
+cudaError_t launch_fp64_rescue(const Fp64LaunchArgs& a);
+size_t fp64_smem_bytes();
+size_t fp64_scratch_bytes_per_row();  // per warp, per border row
+const void* fp64_kernel();
+int fp64_tile();
+
+// Preparation kernels.
+cudaError_t launch_pack(const PrepArgs& a, int grid, cudaStream_t s);
+cudaError_t launch_binning(BinArgs a, int grid, cudaStream_t s, const int* per_task_dev,
+                           const int* config_dev, Schedule* sched, int nranks);
+
+// FP32 FFMA throughput probe used to measure the roofline denominator:
+// `iters` dependent-chain-free FMAs per thread over grid x 256 threads.
+cudaError_t launch_ffma_peak(float* out, int grid, int iters, cudaStream_t s);
+
+}  // namespace phmm

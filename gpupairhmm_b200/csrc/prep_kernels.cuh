@@ -1,0 +1,205 @@
+// Batch preparation kernels: pack reads and haplotypes into the HBM layout
+// of device_common.cuh, then build the sorted work list.
+//
+// Work list: every pair gets a bin  (bucket rank, 4095 - min(H, 4095))  so that
+// an exclusive scan over bins followed by an atomic scatter sorts the pairs by
+// tile bucket (largest tiles first) and, inside a bucket, by haplotype length
+// descending.  Warps of the persistent kernel then take consecutive items, so
+// the groups of a warp have nearly equal haplotype lengths (little idle work)
+// and the longest pairs start first (short tail).  The order of pairs with the
+// same bin is not deterministic; each pair still writes its own output slot,
+// so results are.
+#pragma once
+
+#include "device_common.cuh"
+
+namespace phmm {
+
+constexpr int kHBins = 4096;     // haplotype-length classes per bucket
+constexpr int kMaxBuckets = 48;
+
+struct PrepArgs {
+    // caller arrays (device)
+    const uint8_t* read_bases;
+    const uint8_t* base_quals;
+    const uint8_t* ins_quals;
+    const uint8_t* del_quals;
+    const int64_t* read_offsets;
+    const int32_t* read_lengths;
+    const uint8_t* hap_bases;
+    const int64_t* hap_offsets;
+    const int32_t* hap_lengths;
+    // index arrays (device, computed on the host)
+    const int32_t* read_record;     // [num_reads]
+    const int32_t* read_local;      // [num_reads] read index inside its record
+    const int32_t* rec_haps;        // [num_records] H
+    const int64_t* rec_hap_base;    // [num_records]
+    const int64_t* rec_pair_base;   // [num_records]
+    const int64_t* read_start;      // [num_reads] packed start (positions)
+    const int64_t* hap_start;       // [num_haps] packed start (bytes)
+    int64_t num_reads;
+    int64_t num_haps;
+    // outputs
+    uint32_t* read_pack;
+    uint8_t* hap_code;
+};
+
+#ifdef PHMM_PREP_KERNELS_IMPL
+// warp per read
+__global__ void pack_reads_kernel(PrepArgs a) {
+    const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    for (int64_t i = warp; i < a.num_reads; i += nwarps) {
+        const int L = a.read_lengths[i];
+        const int Lp = (L + 3) & ~3;
+        const int64_t src = a.read_offsets[i];
+        uint32_t* dst = a.read_pack + a.read_start[i];
+        for (int c = lane; c < Lp; c += 32) {
+            uint32_t w = 4u;
+            if (c < L) {
+                const uint32_t x = code_of(a.read_bases[src + c]);
+                uint32_t bq = a.base_quals[src + c], iq = a.ins_quals[src + c], dq = a.del_quals[src + c];
+                bq = bq > 127u ? 127u : bq;
+                iq = iq > 127u ? 127u : iq;
+                dq = dq > 127u ? 127u : dq;
+                w = x | (bq << 8) | (iq << 16) | (dq << 24);
+            }
+            dst[c] = w;
+        }
+    }
+}
+
+// warp per haplotype; pads to 16 bytes with code 4
+__global__ void pack_haps_kernel(PrepArgs a) {
+    const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    for (int64_t i = warp; i < a.num_haps; i += nwarps) {
+        const int H = a.hap_lengths[i];
+        const int Hp = (H + 15) & ~15;
+        const int64_t src = a.hap_offsets[i];
+        uint8_t* dst = a.hap_code + a.hap_start[i];
+        for (int c = lane; c < Hp; c += 32) dst[c] = c < H ? (uint8_t)code_of(a.hap_bases[src + c]) : (uint8_t)4;
+    }
+}
+
+#endif  // PHMM_PREP_KERNELS_IMPL
+
+struct BinArgs {
+    const int32_t* read_lengths;
+    const int32_t* hap_lengths;
+    const int32_t* read_record;
+    const int32_t* read_local;
+    const int32_t* rec_haps;
+    const int64_t* rec_hap_base;
+    const int64_t* rec_pair_base;
+    int64_t num_reads;
+    int nbuckets;
+    int hbins;                      // kHBins (engine) or 1 (plain)
+    const int32_t* bucket_max_len;  // [nbuckets] inclusive upper bound on L, ascending
+    const int32_t* bucket_rank;     // [nbuckets] bin-major position of each bucket
+    unsigned int* hist;             // [nbuckets * hbins]
+    unsigned long long* cursor;     // [nbuckets * hbins] scatter positions
+    Task* items;
+};
+
+__device__ __forceinline__ int bucket_of(int L, const int32_t* bmax, int nb) {
+    int b = 0;
+    while (b < nb - 1 && L > bmax[b]) ++b;
+    return b;
+}
+
+__device__ __forceinline__ int bin_of(const BinArgs& a, int L, int H) {
+    const int b = bucket_of(L, a.bucket_max_len, a.nbuckets);
+    const int hc = a.hbins > 1 ? (a.hbins - 1 - (H < a.hbins - 1 ? H : a.hbins - 1)) : 0;
+    return a.bucket_rank[b] * a.hbins + hc;
+}
+
+#ifdef PHMM_PREP_KERNELS_IMPL
+// thread per read: histogram of (bucket, H class)
+__global__ void bin_count_kernel(BinArgs a) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < a.num_reads;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const int L = a.read_lengths[i];
+        const int g = a.read_record[i];
+        const int nh = a.rec_haps[g];
+        const int64_t hb = a.rec_hap_base[g];
+        for (int h = 0; h < nh; ++h) atomicAdd(&a.hist[bin_of(a, L, a.hap_lengths[hb + h])], 1u);
+    }
+}
+
+// thread per read: scatter items into their sorted slots
+__global__ void bin_scatter_kernel(BinArgs a) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < a.num_reads;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const int L = a.read_lengths[i];
+        const int g = a.read_record[i];
+        const int nh = a.rec_haps[g];
+        const int64_t hb = a.rec_hap_base[g];
+        const int64_t ob = a.rec_pair_base[g] + (int64_t)a.read_local[i] * nh;
+        for (int h = 0; h < nh; ++h) {
+            const int bin = bin_of(a, L, a.hap_lengths[hb + h]);
+            const unsigned long long pos = atomicAdd(&a.cursor[bin], 1ull);
+            a.items[pos] = Task{(int32_t)i, (int32_t)(hb + h), ob + h};
+        }
+    }
+}
+
+// single-block exclusive scan of the histogram into cursor (n up to a few 1e5)
+__global__ void hist_scan_kernel(const unsigned int* hist, unsigned long long* cursor, int n) {
+    __shared__ unsigned long long part[1024];
+    const int tid = threadIdx.x;
+    const int per = (n + blockDim.x - 1) / blockDim.x;
+    const int b = tid * per;
+    const int e = b + per < n ? b + per : n;
+    unsigned long long s = 0;
+    for (int i = b; i < e; ++i) s += hist[i];
+    part[tid] = s;
+    __syncthreads();
+    if (tid == 0) {
+        unsigned long long run = 0;
+        for (int i = 0; i < (int)blockDim.x; ++i) { const unsigned long long x = part[i]; part[i] = run; run += x; }
+    }
+    __syncthreads();
+    unsigned long long run = part[tid];
+    for (int i = b; i < e; ++i) { cursor[i] = run; run += hist[i]; }
+}
+
+#endif  // PHMM_PREP_KERNELS_IMPL
+
+// Per-rank item ranges and warp-task ranges for the persistent kernel.
+struct Schedule {
+    int nranks;
+    int total_tasks_hi;                       // unused padding
+    long long total_tasks;
+    long long item_begin[kMaxBuckets + 1];    // by rank
+    long long task_begin[kMaxBuckets + 1];    // by rank
+    int per_task[kMaxBuckets];                // items per warp task, by rank
+    int config[kMaxBuckets];                  // kernel config id, by rank
+};
+
+#ifdef PHMM_PREP_KERNELS_IMPL
+// one thread: cursor holds bin starts (before scatter); derive the schedule
+__global__ void schedule_kernel(const unsigned long long* bin_start, const unsigned int* hist, int nranks,
+                                int hbins, const int* per_task, const int* config, Schedule* s) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    long long tasks = 0;
+    s->nranks = nranks;
+    for (int r = 0; r < nranks; ++r) {
+        const long long b0 = (long long)bin_start[r * hbins];
+        const long long last = (long long)bin_start[(r + 1) * hbins - 1] + hist[(r + 1) * hbins - 1];
+        s->item_begin[r] = b0;
+        s->task_begin[r] = tasks;
+        s->per_task[r] = per_task[r];
+        s->config[r] = config[r];
+        const long long n = last - b0;
+        tasks += (n + per_task[r] - 1) / per_task[r];
+        if (r == nranks - 1) s->item_begin[nranks] = last;
+    }
+    s->task_begin[nranks] = tasks;
+    s->total_tasks = tasks;
+}
+#endif  // PHMM_PREP_KERNELS_IMPL
+
+}  // namespace phmm

@@ -1,0 +1,246 @@
+#include <algorithm>
+#include <cstring>
+
+#include "serving.hpp"
+
+namespace phmm {
+
+namespace {
+constexpr int64_t kDefaultBudget = int64_t(40) << 30;  // 40 GiB
+constexpr int64_t kMaxBatchPairs = int64_t(4) << 20;   // cap on pairs merged into one batch
+}  // namespace
+
+ServingQueue::ServingQueue(Engine& parent) : parent_(parent) {
+    // the parent's options carry the budget; each slot gets an equal share
+    const int64_t budget = parent.budget_bytes() > 0 ? parent.budget_bytes() : kDefaultBudget;
+    budget_per_slot_ = budget / kSlots;
+}
+
+ServingQueue::~ServingQueue() {
+    {
+        std::lock_guard<std::mutex> lk(mu_);
+        stop_ = true;
+    }
+    cv_work_.notify_all();
+    for (auto& t : threads_) t.join();
+}
+
+int64_t ServingQueue::estimate_device_bytes(const Region& r) {
+    // inputs (4 byte arrays + haplotypes), packed copies, work items, rescue
+    // list and scores, plus the per-read/per-haplotype index arrays
+    const int64_t reads = (int64_t)r.read_len.size(), haps = (int64_t)r.hap_len.size();
+    int64_t pos = 0, hb = 0;
+    for (int32_t L : r.read_len) pos += (L + 3) & ~3;
+    for (int32_t H : r.hap_len) hb += (H + 15) & ~15;
+    return 4 * (int64_t)r.read_bases.size() + 2 * (int64_t)r.hap_bases.size() + 4 * pos + hb +
+           r.pairs * (16 + 16 + 4) + reads * 32 + haps * 24 + 4096;
+}
+
+pairhmm_status_t ServingQueue::submit(const pairhmm_batch_t& b, uint64_t* ticket) {
+    BatchIndex x;
+    std::string err;
+    pairhmm_status_t st = Engine::build_index(b, parent_.tile_table(), x, err);
+    if (st != PAIRHMM_OK) {
+        error_ = err;
+        return st;
+    }
+    if (x.num_reads > 0 && (!b.read_bases || !b.base_quals || !b.ins_quals || !b.del_quals || !b.read_offsets)) {
+        error_ = "null read arrays";
+        return PAIRHMM_ERR_INVALID_ARGUMENT;
+    }
+    if (x.num_haps > 0 && (!b.hap_bases || !b.hap_offsets)) {
+        error_ = "null haplotype arrays";
+        return PAIRHMM_ERR_INVALID_ARGUMENT;
+    }
+    auto r = std::make_shared<Region>();
+    r->rpr.assign(b.reads_per_record, b.reads_per_record + b.num_records);
+    r->hpr.assign(b.haps_per_record, b.haps_per_record + b.num_records);
+    r->read_len.assign(b.read_lengths, b.read_lengths + x.num_reads);
+    r->hap_len.assign(b.hap_lengths, b.hap_lengths + x.num_haps);
+    // compact copy: each read/haplotype stored back to back
+    r->read_off.resize(x.num_reads);
+    r->hap_off.resize(x.num_haps);
+    int64_t total = 0;
+    for (int64_t i = 0; i < x.num_reads; ++i) { r->read_off[i] = total; total += b.read_lengths[i]; }
+    r->read_bases.resize(total);
+    r->bq.resize(total);
+    r->iq.resize(total);
+    r->dq.resize(total);
+    for (int64_t i = 0; i < x.num_reads; ++i) {
+        const int64_t o = b.read_offsets[i], d = r->read_off[i], L = b.read_lengths[i];
+        std::memcpy(&r->read_bases[d], b.read_bases + o, L);
+        std::memcpy(&r->bq[d], b.base_quals + o, L);
+        std::memcpy(&r->iq[d], b.ins_quals + o, L);
+        std::memcpy(&r->dq[d], b.del_quals + o, L);
+    }
+    total = 0;
+    for (int64_t h = 0; h < x.num_haps; ++h) { r->hap_off[h] = total; total += b.hap_lengths[h]; }
+    r->hap_bases.resize(total);
+    for (int64_t h = 0; h < x.num_haps; ++h)
+        std::memcpy(&r->hap_bases[r->hap_off[h]], b.hap_bases + b.hap_offsets[h], b.hap_lengths[h]);
+    r->pairs = x.num_pairs;
+    r->device_bytes = estimate_device_bytes(*r);
+    if (r->device_bytes > budget_per_slot_) {
+        error_ = "region needs more device memory than one batch slot's budget";
+        return PAIRHMM_ERR_BUDGET;
+    }
+    r->t_submit = std::chrono::steady_clock::now();
+    {
+        std::lock_guard<std::mutex> lk(mu_);
+        if (engines_.empty()) {
+            for (int s = 0; s < kSlots; ++s) {
+                pairhmm_options_t o{};
+                o.device = parent_.device();
+                o.mode = PAIRHMM_MODE_ENGINE;
+                o.fp64_rescue = 1;
+                o.use_graphs = 1;
+                auto e = std::make_unique<Engine>(o);
+                pairhmm_status_t is = e->init();
+                if (is == PAIRHMM_OK) is = e->set_tile_table(parent_.tile_table());
+                if (is != PAIRHMM_OK) {
+                    error_ = e->last_error();
+                    engines_.clear();
+                    return is;
+                }
+                engines_.push_back(std::move(e));
+            }
+            for (int s = 0; s < kSlots; ++s) threads_.emplace_back(&ServingQueue::worker, this, s);
+        }
+        r->ticket = next_ticket_++;
+        tickets_[r->ticket] = r;
+        queue_.push_back(r);
+        *ticket = r->ticket;
+    }
+    cv_work_.notify_one();
+    return PAIRHMM_OK;
+}
+
+void ServingQueue::worker(int slot) {
+    Engine& eng = *engines_[slot];
+    for (;;) {
+        std::vector<std::shared_ptr<Region>> take;
+        bool more = false;
+        {
+            std::unique_lock<std::mutex> lk(mu_);
+            cv_work_.wait(lk, [&] { return stop_ || !queue_.empty(); });
+            if (stop_ && queue_.empty()) return;
+            // admission: everything queued that fits this slot's budget
+            int64_t bytes = 0, pairs = 0;
+            while (!queue_.empty()) {
+                const auto& r = queue_.front();
+                if (!take.empty() && (bytes + r->device_bytes > budget_per_slot_ || pairs + r->pairs > kMaxBatchPairs))
+                    break;
+                bytes += r->device_bytes;
+                pairs += r->pairs;
+                take.push_back(r);
+                queue_.pop_front();
+            }
+            more = !queue_.empty();
+        }
+        if (more) cv_work_.notify_one();
+        // merge the regions into one batch
+        std::vector<int32_t> rpr, hpr, rl, hl;
+        std::vector<int64_t> ro, ho;
+        std::vector<uint8_t> rb, bq, iq, dq, hb;
+        for (const auto& r : take) {
+            const int64_t rbase = (int64_t)rb.size(), hbase = (int64_t)hb.size();
+            rpr.insert(rpr.end(), r->rpr.begin(), r->rpr.end());
+            hpr.insert(hpr.end(), r->hpr.begin(), r->hpr.end());
+            rl.insert(rl.end(), r->read_len.begin(), r->read_len.end());
+            hl.insert(hl.end(), r->hap_len.begin(), r->hap_len.end());
+            for (int64_t o : r->read_off) ro.push_back(rbase + o);
+            for (int64_t o : r->hap_off) ho.push_back(hbase + o);
+            rb.insert(rb.end(), r->read_bases.begin(), r->read_bases.end());
+            bq.insert(bq.end(), r->bq.begin(), r->bq.end());
+            iq.insert(iq.end(), r->iq.begin(), r->iq.end());
+            dq.insert(dq.end(), r->dq.begin(), r->dq.end());
+            hb.insert(hb.end(), r->hap_bases.begin(), r->hap_bases.end());
+        }
+        pairhmm_batch_t b{};
+        b.num_records = (int64_t)rpr.size();
+        b.reads_per_record = rpr.data();
+        b.haps_per_record = hpr.data();
+        b.read_bases = rb.data();
+        b.base_quals = bq.data();
+        b.ins_quals = iq.data();
+        b.del_quals = dq.data();
+        b.read_offsets = ro.data();
+        b.read_lengths = rl.data();
+        b.hap_bases = hb.data();
+        b.hap_offsets = ho.data();
+        b.hap_lengths = hl.data();
+        int64_t total_pairs = 0;
+        for (const auto& r : take) total_pairs += r->pairs;
+        std::vector<float> scores((size_t)std::max<int64_t>(total_pairs, 1));
+        const pairhmm_status_t st = eng.compute_host(b, scores.data());
+        const auto now = std::chrono::steady_clock::now();
+        {
+            std::lock_guard<std::mutex> lk(mu_);
+            int64_t off = 0;
+            for (const auto& r : take) {
+                r->status = st;
+                if (st != PAIRHMM_OK) r->error = eng.last_error();
+                else r->scores.assign(scores.begin() + off, scores.begin() + off + r->pairs);
+                off += r->pairs;
+                r->t_done = now;
+                r->done = true;
+            }
+        }
+        cv_done_.notify_all();
+    }
+}
+
+pairhmm_status_t ServingQueue::poll(uint64_t ticket, int32_t* done) {
+    std::lock_guard<std::mutex> lk(mu_);
+    auto it = tickets_.find(ticket);
+    if (it == tickets_.end()) {
+        error_ = "unknown ticket";
+        return PAIRHMM_ERR_NOT_FOUND;
+    }
+    *done = it->second->done ? 1 : 0;
+    return PAIRHMM_OK;
+}
+
+pairhmm_status_t ServingQueue::latency(uint64_t ticket, double* ms) {
+    std::lock_guard<std::mutex> lk(mu_);
+    auto it = tickets_.find(ticket);
+    if (it == tickets_.end()) {
+        error_ = "unknown ticket";
+        return PAIRHMM_ERR_NOT_FOUND;
+    }
+    if (!it->second->done) {
+        error_ = "region not finished";
+        return PAIRHMM_ERR_BUSY;
+    }
+    *ms = std::chrono::duration<double, std::milli>(it->second->t_done - it->second->t_submit).count();
+    return PAIRHMM_OK;
+}
+
+pairhmm_status_t ServingQueue::drain(uint64_t ticket, float* scores, int64_t num_scores, int32_t timeout_ms) {
+    std::unique_lock<std::mutex> lk(mu_);
+    auto it = tickets_.find(ticket);
+    if (it == tickets_.end()) {
+        error_ = "unknown ticket";
+        return PAIRHMM_ERR_NOT_FOUND;
+    }
+    std::shared_ptr<Region> r = it->second;
+    if (timeout_ms < 0) cv_done_.wait(lk, [&] { return r->done; });
+    else if (!cv_done_.wait_for(lk, std::chrono::milliseconds(timeout_ms), [&] { return r->done; })) {
+        error_ = "timed out waiting for the region";
+        return PAIRHMM_ERR_TIMEOUT;
+    }
+    if (r->status != PAIRHMM_OK) {
+        error_ = r->error;
+        tickets_.erase(it);
+        return r->status;
+    }
+    if (num_scores < r->pairs) {
+        error_ = "score buffer smaller than the region's pair count";
+        return PAIRHMM_ERR_INVALID_ARGUMENT;
+    }
+    std::copy(r->scores.begin(), r->scores.end(), scores);
+    tickets_.erase(it);
+    return PAIRHMM_OK;
+}
+
+}  // namespace phmm

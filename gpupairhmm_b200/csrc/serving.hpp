@@ -1,0 +1,72 @@
+// Continuous-batching request loop (no counterpart in the reference, which
+// only processes whole files: gpuworker.cuh:435-471).
+//
+// submit() copies a region (one or more records) into host memory and queues
+// it.  kSlots worker threads each own an Engine (own stream and device
+// buffers); a worker that becomes free takes every queued region that fits its
+// share of the device budget, merges them into one batch, runs it, and
+// completes the tickets.  While one slot's batch runs on the GPU the next slot
+// is already admitting, uploading and launching, so the work of regions that
+// arrive while others are on the device overlaps with them.
+#pragma once
+
+#include <chrono>
+#include <condition_variable>
+#include <cstdint>
+#include <deque>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "engine.hpp"
+
+namespace phmm {
+
+class ServingQueue {
+public:
+    explicit ServingQueue(Engine& parent);
+    ~ServingQueue();
+
+    pairhmm_status_t submit(const pairhmm_batch_t& region, uint64_t* ticket);
+    pairhmm_status_t poll(uint64_t ticket, int32_t* done);
+    pairhmm_status_t drain(uint64_t ticket, float* scores, int64_t num_scores, int32_t timeout_ms);
+    pairhmm_status_t latency(uint64_t ticket, double* ms);
+    const std::string& last_error() const { return error_; }
+
+    static constexpr int kSlots = 2;
+
+private:
+    struct Region {
+        uint64_t ticket = 0;
+        std::vector<int32_t> rpr, hpr, read_len, hap_len;
+        std::vector<int64_t> read_off, hap_off;
+        std::vector<uint8_t> read_bases, bq, iq, dq, hap_bases;
+        int64_t pairs = 0;
+        int64_t device_bytes = 0;
+        std::chrono::steady_clock::time_point t_submit, t_done;
+        std::vector<float> scores;
+        bool done = false;
+        pairhmm_status_t status = PAIRHMM_OK;
+        std::string error;
+    };
+
+    void worker(int slot);
+    static int64_t estimate_device_bytes(const Region& r);
+
+    Engine& parent_;
+    int64_t budget_per_slot_ = 0;
+    std::vector<std::unique_ptr<Engine>> engines_;
+    std::vector<std::thread> threads_;
+    std::mutex mu_;
+    std::condition_variable cv_work_, cv_done_;
+    std::deque<std::shared_ptr<Region>> queue_;
+    std::map<uint64_t, std::shared_ptr<Region>> tickets_;
+    uint64_t next_ticket_ = 1;
+    bool stop_ = false;
+    std::string error_;
+};
+
+}  // namespace phmm

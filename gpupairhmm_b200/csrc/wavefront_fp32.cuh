@@ -1,0 +1,271 @@
+// FP32 anti-diagonal wavefront for the PairHMM forward recurrence.
+//
+// Work split (one warp = 32/G groups, one pair per group):
+//   lane t of a group owns R consecutive read positions c = tile*T + t*R + r,
+//   T = G*R.  Haplotype positions stream through the group: at step k lane t
+//   works on haplotype row j = k - t, so the group sweeps one anti-diagonal
+//   band per step.  The last N, D and I of a lane move one lane up with
+//   __shfl_up_sync each step (the boundary column hand-off).
+//
+// Recurrence (the algebra of pairhmm_kernels.cuh:1417-1651 and
+// gpuworker.cuh:1048-1075):
+//     M(j,c) = lambda(h_j,c) * (alpha_c*M(j-1,c-1) + beta*(I(j-1,c-1) + D(j-1,c-1)))
+//     I(j,c) = delta_c*M(j,c-1) + eps*I(j,c-1)
+//     D(j,c) = sigma_c*M(j-1,c) + eps*D(j-1,c)
+// stored in rescaled variables that fold every constant factor into tables:
+//     N = alpha_{c+1}*M,  It = beta*I,  Dt = beta*D
+//     N(j,c)  = lam'(h_j,c) * (N(j-1,c-1) + It(j-1,c-1) + Dt(j-1,c-1)),  lam' = alpha_{c+1}*lambda
+//     It(j,c) = d'_c*N(j,c-1) + eps_c*It(j,c-1),                        d'   = beta*delta_c/alpha_c
+//     Dt(j,c) = s'_c*N(j-1,c) + eps*Dt(j-1,c),                          s'   = beta*sigma_c/alpha_{c+1}
+// 7 FP32 instructions per cell (FADD+FADD+FMUL, FMUL+FFMA, FMUL+FFMA), only
+// lam' (4 bytes per cell) comes from shared memory, and the per-position
+// registers are N, Dt, d', s', eps (5R).  Pairs with |alpha| < 2^-8 somewhere
+// (ins+del quality around 3 or below) cannot use the division; they are
+// flagged for the FP64 pass, which runs the untransformed recurrence.
+// I is computed one anti-diagonal behind M, as in the reference
+// (pairhmm_kernels.cuh:1423-1426).
+//
+// Result: the position after the read end gets alpha = 1, d' = beta, eps = 1
+// and later positions d' = 0, eps = 1, so the lane's last It carries
+// beta*(M+I)(j, L-1) (the reference's trick, pairhmm_kernels.cuh:1307-1331,
+// with beta folded in).  Summing over j gives beta * sum_j (M+I)(L-1,j).
+//
+// lam' table: each thread owns 5 x R floats in shared memory, laid out as
+// [hap code][R/4][32 lanes] float4, so a warp-wide 16-byte load touches 32
+// consecutive float4s whatever codes the lanes hold (no bank conflicts) and a
+// thread only reads what it wrote (no synchronisation).
+//
+// Reads longer than T (MT = true) run as several tiles; the last lane of tile
+// i writes (N, Dt, It) of its last position for every haplotype row into a
+// per-group scratch border, which lane 0 of tile i+1 reads as its left
+// boundary (pairhmm_kernels.cuh:2167-3272 does the same with 512-row tiles).
+#pragma once
+
+#include "device_common.cuh"
+
+namespace phmm {
+
+template <int G, int R, bool MT>
+struct Fp32Wavefront {
+    static_assert(R % 4 == 0 && R >= 4, "R must be a multiple of 4");
+    static_assert(G == 4 || G == 8 || G == 16 || G == 32, "G must divide the warp");
+    static constexpr int NG = 32 / G;   // pairs per warp
+    static constexpr int T = G * R;     // read positions per tile
+    static constexpr int Q = R / 4;     // float4 per thread per table row
+    static constexpr int kTableFloat4 = 5 * Q * 32;  // per warp
+
+    // tasks: the warp's ntask (<= NG) work items.  wtab: this warp's table
+    // (kTableFloat4 float4).  ph: 128-entry probability table (shared).
+    // scratch: this warp's border storage, NG groups x 2 buffers x rows float4.
+    __device__ static void run(const DevView& v, const Task* tasks, int ntask, float4* wtab,
+                               const float* ph, float4* scratch, int64_t rows) {
+        const int lane = threadIdx.x & 31;
+        const int grp = lane / G;
+        const int t = lane - grp * G;
+        const bool active = grp < ntask;
+        const Task task = tasks[active ? grp : 0];
+        const int L = v.read_len[task.read];
+        const int H = v.hap_len[task.hap];
+        const bool valid = active && L >= 1 && H >= 1;
+        const int Lc = L >= 1 ? L : 1;
+        const int Hc = H >= 1 ? H : 1;
+        const int ntiles = MT ? (Lc + T - 1) / T : 1;
+        const int nt_warp = MT ? (int)__reduce_max_sync(kFullMask, (unsigned)ntiles) : 1;
+
+        const uint32_t* rpack = v.read_pack + v.read_start[task.read];
+        const uint32_t* hw = reinterpret_cast<const uint32_t*>(v.hap_code + v.hap_start[task.hap]);
+        const float Dbound = kBeta * (kScale / (float)Hc);
+
+        float acc = 0.f;
+        int rlane = -1;          // lane (in group) that holds the result
+        bool degenerate = false; // some |alpha| < kMinAlpha: FP64 pass recomputes the pair
+
+        for (int tile = 0; tile < nt_warp; ++tile) {
+            const bool tile_live = valid && tile < ntiles;
+            const bool last = tile == ntiles - 1;
+            const int p0 = tile * T + t * R;
+
+            // ---------------- per-tile parameters (O(R) per lane) ----------------
+            // alpha of the position after this lane's last one (next lane / tile)
+            float alpha_next;
+            {
+                const int cn = p0 + R;
+                alpha_next = 1.0f;
+                if (cn < Lc) {
+                    const uint32_t wn = __ldg(rpack + cn);
+                    alpha_next = 1.0f - (ph[(wn >> 16) & 0x7fu] + ph[(wn >> 24) & 0x7fu]);
+                }
+            }
+            float dlt[R], sig[R], eps[R];
+            float N[R], D[R];
+            float a_cur[R];
+#pragma unroll
+            for (int q = 0; q < Q; ++q) {
+                uint4 w = make_uint4(0u, 0u, 0u, 0u);
+                if (p0 + 4 * q < Lc) w = __ldg(reinterpret_cast<const uint4*>(rpack + p0 + 4 * q));
+                const uint32_t ws[4] = {w.x, w.y, w.z, w.w};
+#pragma unroll
+                for (int s = 0; s < 4; ++s) {
+                    const int r = 4 * q + s;
+                    const float d = ph[(ws[s] >> 16) & 0x7fu];
+                    const float sg = ph[(ws[s] >> 24) & 0x7fu];
+                    a_cur[r] = (p0 + r < L) ? 1.0f - (d + sg) : 1.0f;  // pairhmm_kernels.cuh:1336
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < Q; ++q) {
+                uint4 w = make_uint4(0u, 0u, 0u, 0u);
+                if (p0 + 4 * q < Lc) w = __ldg(reinterpret_cast<const uint4*>(rpack + p0 + 4 * q));
+                const uint32_t ws[4] = {w.x, w.y, w.z, w.w};
+                float lam[5][4];
+#pragma unroll
+                for (int s = 0; s < 4; ++s) {
+                    const int r = 4 * q + s;
+                    const int c = p0 + r;
+                    const uint32_t x = ws[s] & 0xffu;
+                    const float p = ph[(ws[s] >> 8) & 0x7fu];
+                    const float d = ph[(ws[s] >> 16) & 0x7fu];
+                    const float sg = ph[(ws[s] >> 24) & 0x7fu];
+                    const bool in = c < L;
+                    const float an = (r + 1 < R) ? a_cur[r + 1 < R ? r + 1 : r] : alpha_next;
+                    const float lm = 1.0f - p;      // pairhmm_kernels.cuh:1244
+                    const float lx = p / 3.0f;      // pairhmm_kernels.cuh:1250
+#pragma unroll
+                    for (int h = 0; h < 5; ++h)
+                        lam[h][s] = in ? an * ((x == 4u || h == 4 || x == (uint32_t)h) ? lm : lx) : 0.0f;
+                    if (in && !(fabsf(a_cur[r]) >= kMinAlpha)) degenerate = true;
+                    dlt[r] = in ? (kBeta * d) / a_cur[r] : (c == L ? kBeta : 0.0f);
+                    sig[r] = (kBeta * sg) / an;
+                    eps[r] = in ? kEps : 1.0f;
+                    N[r] = 0.0f;
+                    D[r] = 0.0f;
+                }
+#pragma unroll
+                for (int h = 0; h < 5; ++h)
+                    wtab[(h * Q + q) * 32 + lane] = make_float4(lam[h][0], lam[h][1], lam[h][2], lam[h][3]);
+            }
+
+            // ---------------- steps of this tile ----------------
+            int t_res = 0, r_res = 0;
+            if (last) {
+                const int rel = Lc - 1 - tile * T;
+                t_res = rel / R;
+                r_res = rel - t_res * R;
+            }
+            // last step index that matters for this group
+            const int kg = last ? (Hc + t_res) : (Hc + G - 1);
+            const bool res_lane = tile_live && last && t == t_res;
+            const bool addM = r_res == R - 1;
+            if (res_lane) rlane = t;
+            const int kmax = (int)__reduce_max_sync(kFullMask, (unsigned)(tile_live ? kg : 0));
+            const int K = (kmax + 1 + 3) & ~3;
+
+            float Ml = 0.f, Dl = 0.f, Mul = 0.f, Dul = 0.f, Iul = 0.f;
+            if (t == 0 && tile == 0) { Dl = Dbound; Dul = Dbound; }
+            int h = 4;
+
+            // border in/out (MT only)
+            float4* ein = nullptr;
+            float4* eout = nullptr;
+            float4 bcur = make_float4(0.f, 0.f, 0.f, 0.f), bnext = bcur;
+            if (MT) {
+                float4* gbase = scratch + (int64_t)grp * 2 * rows;
+                if (tile > 0) {
+                    ein = gbase + ((tile - 1) & 1) * rows;
+                    if (t < rows) bcur = __ldcg(ein + t);
+                    if (G + t < rows) bnext = __ldcg(ein + G + t);
+                }
+                eout = gbase + (tile & 1) * rows;
+            }
+            const bool writer = MT && tile_live && !last && t == G - 1;
+
+            // code words of this group's haplotype; a group whose haplotype is
+            // shorter than the warp's step count keeps re-reading its last word
+            // (any code there is harmless: those rows are past the haplotype)
+            const int wlast = ((Hc + 15) & ~15) / 4 - 1;
+            uint32_t wcur = __ldg(hw);
+            uint32_t wnext = __ldg(hw + 1);
+            for (int k0 = 0; k0 < K; k0 += 4) {
+                const uint32_t wpref = __ldg(hw + min_i((k0 >> 2) + 2, wlast));
+#pragma unroll
+                for (int s = 0; s < 4; ++s) {
+                    const int k = k0 + s;
+                    int hn = __shfl_up_sync(kFullMask, h, 1, G);
+                    if (t == 0) hn = (int)((wcur >> (8 * s)) & 0xffu);
+                    h = hn;
+                    const float4* trow = wtab + h * (Q * 32) + lane;
+                    float Ndiag = Mul, Idiag = Iul, Xdiag = Iul + Dul;
+#pragma unroll
+                    for (int q = 0; q < Q; ++q) {
+                        const float4 lam = trow[q * 32];
+                        const float ls[4] = {lam.x, lam.y, lam.z, lam.w};
+#pragma unroll
+                        for (int u = 0; u < 4; ++u) {
+                            const int r = 4 * q + u;
+                            const float Nold = N[r];
+                            const float Dold = D[r];
+                            N[r] = ls[u] * (Ndiag + Xdiag);
+                            D[r] = fmaf(sig[r], Nold, kEps * Dold);
+                            const float In = fmaf(dlt[r], Ndiag, eps[r] * Idiag);
+                            Ndiag = Nold;
+                            Idiag = In;
+                            Xdiag = In + Dold;
+                        }
+                    }
+                    // result (row k - t_res): It(j-1) at the lane end, plus beta*M(j) when
+                    // the read ends on the lane's last register
+                    if (res_lane && k <= kg) {
+                        acc += Idiag;
+                        if (addM && k < kg) acc = fmaf(kBeta, N[R - 1], acc);
+                    }
+                    if (MT && writer) {
+                        const int j = k - (G - 1);
+                        if (j >= 0 && j < Hc)
+                            *reinterpret_cast<float2*>(eout + j) = make_float2(N[R - 1], D[R - 1]);
+                        if (j >= 1 && j - 1 < Hc) reinterpret_cast<float*>(eout + (j - 1))[2] = Idiag;
+                    }
+                    // boundary hand-off
+                    Mul = Ml;
+                    Dul = Dl;
+                    Ml = __shfl_up_sync(kFullMask, N[R - 1], 1, G);
+                    Dl = __shfl_up_sync(kFullMask, D[R - 1], 1, G);
+                    Iul = __shfl_up_sync(kFullMask, Idiag, 1, G);
+                    if (MT && tile > 0) {
+                        const int src = k & (G - 1);
+                        const float bx = __shfl_sync(kFullMask, bcur.x, src, G);
+                        const float by = __shfl_sync(kFullMask, bcur.y, src, G);
+                        const float bz = __shfl_sync(kFullMask, bcur.z, src, G);
+                        if (t == 0) { Ml = bx; Dl = by; Iul = bz; }
+                        if (src == G - 1) {
+                            bcur = bnext;
+                            const int64_t idx = (int64_t)k + 1 + G + t;
+                            bnext = idx < rows ? __ldcg(ein + idx) : make_float4(0.f, 0.f, 0.f, 0.f);
+                        }
+                    } else if (t == 0) {
+                        Ml = 0.f;
+                        Dl = Dbound;
+                        Iul = 0.f;
+                    }
+                }
+                wcur = wnext;
+                wnext = wpref;
+            }
+            __syncwarp();
+        }
+
+        // any lane of the group saw a degenerate alpha
+        const unsigned dmask = __ballot_sync(kFullMask, degenerate);
+        const unsigned gmask = (G == 32 ? kFullMask : ((1u << G) - 1u)) << (grp * G);
+        degenerate = (dmask & gmask) != 0u;
+        if (valid && t == rlane) {
+            const float res = log10f(acc) - (log10f(kScale) + log10f(kBeta));
+            v.scores[task.out] = res;
+            if (degenerate || (v.rescue_enabled && !(acc >= kRescueThreshold && acc <= FLT_MAX))) {
+                const unsigned long long slot = atomicAdd(v.rescue_count, 1ull);
+                v.rescue[slot] = task;
+            }
+        }
+    }
+};
+
+}  // namespace phmm

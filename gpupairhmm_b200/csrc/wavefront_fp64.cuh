@@ -1,0 +1,223 @@
+// FP64 rescue pass: the same wavefront in double precision for the pairs
+// whose FP32 result fell below the underflow threshold.
+//
+// Range: along the read the forward values of an unrelated pair fall by about
+// 10^-3.4 per position (10^-850 over 250 bp), beyond even a pre-scaled double.
+// Every lane therefore stores its values as  true * 2^e  with its own integer
+// exponent e.  Every 8 steps a lane renormalises its registers by an exact
+// power of two, and every value handed to the next lane travels with the
+// sender's exponent; the receiver multiplies it by 2^(e_recv - e_send).  The
+// result lane keeps its accumulator in its own scale and renormalises it with
+// its registers, so the result is  log10(acc) - e*log10(2) - log10(beta*FLT_MAX/16).
+// Values more than 2^1022 below the largest value of their lane are dropped;
+// their contribution to the result is below that factor too.
+//
+// One warp (G = 32 lanes, R doubles per lane, T = 32*R positions per tile) per
+// pair.  Reads longer than T run tile after tile; the last lane's
+// (M, Dt, It, exponents) per haplotype row go through a global border buffer,
+// staged through a 32-entry shared ring for lane 0 of the next tile.
+#pragma once
+
+#include "device_common.cuh"
+
+namespace phmm {
+
+struct Border64 {
+    double m, d, i;
+    int e;   // exponent of m and d (row j)
+    int ei;  // exponent of i (row j)
+};
+static_assert(sizeof(Border64) == 32, "Border64 is 32 bytes");
+
+// 2^k as a double for k clamped to the normal range (exact power of two)
+__device__ __forceinline__ double pow2i(int k) {
+    k = k < -1022 ? -1022 : (k > 1023 ? 1023 : k);
+    return __longlong_as_double((long long)(k + 1023) << 52);
+}
+
+template <int R>
+struct Fp64Wavefront {
+    static_assert(R % 2 == 0, "R must be even");
+    static constexpr int G = 32;
+    static constexpr int T = G * R;
+    static constexpr int Q = R / 2;                 // double2 per thread per table row
+    static constexpr int kTableDouble2 = 5 * Q * 32;  // per warp
+    static constexpr int kRing = 32;
+
+    // One pair per warp.  wtab: this warp's lambda table; ring: kRing entries
+    // of shared memory; scratch: this warp's 2 x rows Border64 in global memory.
+    __device__ static void run(const DevView& v, const Task& task, const float* ph, double2* wtab,
+                               Border64* ring, Border64* scratch, int64_t rows) {
+        const int t = threadIdx.x & 31;
+        const int L = v.read_len[task.read];
+        const int H = v.hap_len[task.hap];
+        if (L < 1 || H < 1) return;  // warp-uniform
+        const int ntiles = (L + T - 1) / T;
+        const uint32_t* rpack = v.read_pack + v.read_start[task.read];
+        const uint32_t* hw = reinterpret_cast<const uint32_t*>(v.hap_code + v.hap_start[task.hap]);
+        const double beta = (double)kBeta;
+        const double epsd = (double)kEps;
+        const double Dbound = beta * (double)(kScale / (float)H);
+
+        double acc = 0.0;
+        int e = 0;
+
+        for (int tile = 0; tile < ntiles; ++tile) {
+            const bool last = tile == ntiles - 1;
+            const int p0 = tile * T + t * R;
+            double alpha[R], dlt[R], sig[R], eps[R], M[R], D[R];
+#pragma unroll
+            for (int q = 0; q < Q; ++q) {
+                double lam[5][2];
+#pragma unroll
+                for (int s = 0; s < 2; ++s) {
+                    const int r = 2 * q + s;
+                    const int c = p0 + r;
+                    const bool in = c < L;
+                    const uint32_t w = in ? __ldg(rpack + c) : 0u;
+                    const uint32_t x = w & 0xffu;
+                    const float p = ph[(w >> 8) & 0x7fu];
+                    const float d = ph[(w >> 16) & 0x7fu];
+                    const float sg = ph[(w >> 24) & 0x7fu];
+                    const double lm = (double)(1.0f - p);
+                    const double lx = (double)(p / 3.0f);
+#pragma unroll
+                    for (int h = 0; h < 5; ++h)
+                        lam[h][s] = in ? ((x == 4u || h == 4 || x == (uint32_t)h) ? lm : lx) : 0.0;
+                    alpha[r] = (double)(1.0f - (d + sg));
+                    dlt[r] = in ? beta * (double)d : (c == L ? beta : 0.0);
+                    sig[r] = beta * (double)sg;
+                    eps[r] = in ? epsd : 1.0;
+                    M[r] = 0.0;
+                    D[r] = 0.0;
+                }
+#pragma unroll
+                for (int h = 0; h < 5; ++h) wtab[(h * Q + q) * 32 + t] = make_double2(lam[h][0], lam[h][1]);
+            }
+            e = 0;
+            int t_res = 0, r_res = 0;
+            if (last) {
+                const int rel = L - 1 - tile * T;
+                t_res = rel / R;
+                r_res = rel - t_res * R;
+            }
+            const int kg = last ? H + t_res : H + G - 1;
+            const bool res_lane = last && t == t_res;
+            const bool addM = r_res == R - 1;
+            const int K = (kg + 1 + 3) & ~3;
+
+            double Ml = 0.0, Dl = 0.0, Mul = 0.0, Dul = 0.0, Iul = 0.0;
+            int eMl = 0, eMul = 0, eIul = 0;
+            if (t == 0 && tile == 0) { Dl = Dbound; Dul = Dbound; }
+            const Border64* ein = scratch + ((tile - 1) & 1) * rows;
+            Border64* eout = scratch + (tile & 1) * rows;
+            const bool writer = !last && t == G - 1;
+            Border64 nb{0.0, 0.0, 0.0, 0, 0};
+            if (tile > 0 && t < rows) nb = ein[t];
+            int h = 4;
+
+            const int wlast = ((H + 15) & ~15) / 4 - 1;
+            uint32_t wcur = __ldg(hw);
+            uint32_t wnext = __ldg(hw + 1);
+            for (int k0 = 0; k0 < K; k0 += 4) {
+                const uint32_t wpref = __ldg(hw + min_i((k0 >> 2) + 2, wlast));
+                if (tile > 0 && (k0 & (kRing - 1)) == 0) {
+                    __syncwarp();
+                    ring[t] = nb;
+                    __syncwarp();
+                    const int64_t idx = (int64_t)k0 + kRing + t;
+                    if (idx < rows) nb = ein[idx];
+                }
+#pragma unroll
+                for (int s = 0; s < 4; ++s) {
+                    const int k = k0 + s;
+                    int hn = __shfl_up_sync(kFullMask, h, 1);
+                    if (t == 0) hn = (int)((wcur >> (8 * s)) & 0xffu);
+                    h = hn;
+                    const double2* trow = wtab + h * (Q * 32) + t;
+                    const double fM = pow2i(e - eMul);
+                    const double fI = pow2i(e - eIul);
+                    double Mdiag = Mul * fM;
+                    double Idiag = Iul * fI;
+                    double Xdiag = fma(Dul, fM, Idiag);
+#pragma unroll
+                    for (int q = 0; q < Q; ++q) {
+                        const double2 lam = trow[q * 32];
+                        const double ls[2] = {lam.x, lam.y};
+#pragma unroll
+                        for (int u = 0; u < 2; ++u) {
+                            const int r = 2 * q + u;
+                            const double Mold = M[r];
+                            const double Dold = D[r];
+                            M[r] = ls[u] * fma(alpha[r], Mdiag, Xdiag);
+                            D[r] = fma(sig[r], Mold, epsd * Dold);
+                            const double In = fma(dlt[r], Mdiag, eps[r] * Idiag);
+                            Mdiag = Mold;
+                            Idiag = In;
+                            Xdiag = In + Dold;
+                        }
+                    }
+                    if (res_lane && k <= kg) {
+                        acc += Idiag;
+                        if (addM && k < kg) acc = fma(beta, M[R - 1], acc);
+                    }
+                    if (writer) {
+                        const int j = k - (G - 1);
+                        if (j >= 0 && j < H) { eout[j].m = M[R - 1]; eout[j].d = D[R - 1]; eout[j].e = e; }
+                        if (j >= 1 && j - 1 < H) { eout[j - 1].i = Idiag; eout[j - 1].ei = e; }
+                    }
+                    // hand-off: values travel with the sender's exponent
+                    Mul = Ml; Dul = Dl; eMul = eMl;
+                    Ml = __shfl_up_sync(kFullMask, M[R - 1], 1);
+                    Dl = __shfl_up_sync(kFullMask, D[R - 1], 1);
+                    Iul = __shfl_up_sync(kFullMask, Idiag, 1);
+                    const int es = __shfl_up_sync(kFullMask, e, 1);
+                    eMl = es;
+                    eIul = es;
+                    if (t == 0) {
+                        if (tile > 0) {
+                            if (k < H) {
+                                const Border64 b = ring[k & (kRing - 1)];
+                                Ml = b.m; Dl = b.d; eMl = b.e; Iul = b.i; eIul = b.ei;
+                            } else {
+                                Ml = 0.0; Dl = 0.0; Iul = 0.0; eMl = 0; eIul = 0;
+                            }
+                        } else {
+                            Ml = 0.0; Dl = Dbound; Iul = 0.0; eMl = 0; eIul = 0;
+                        }
+                    }
+                    // renormalise this lane every 8 steps (exact powers of two)
+                    if ((k & 7) == 7) {
+                        double mx = res_lane ? fabs(acc) : 0.0;
+#pragma unroll
+                        for (int r = 0; r < R; ++r) mx = fmax(mx, fmax(fabs(M[r]), fabs(D[r])));
+                        if (mx > 0.0) {
+                            const int fe = ilogb(mx);
+                            if (fe > 64 || fe < -64) {
+                                const int kk = -fe < -1022 ? -1022 : (-fe > 1023 ? 1023 : -fe);
+                                const double f = pow2i(kk);
+#pragma unroll
+                                for (int r = 0; r < R; ++r) { M[r] *= f; D[r] *= f; }
+                                acc *= f;
+                                e += kk;
+                            }
+                        }
+                    }
+                }
+                wcur = wnext;
+                wnext = wpref;
+            }
+            __syncwarp();
+        }
+        const int rel = L - 1 - (ntiles - 1) * T;
+        if (t == rel / R) {
+            double res = -INFINITY;
+            if (acc > 0.0)
+                res = log10(acc) - (double)e * 0.30102999566398119521 - log10((double)kScale) -
+                      log10((double)kBeta);
+            v.scores[task.out] = (float)res;
+        }
+    }
+};
+
+}  // namespace phmm

@@ -1,0 +1,204 @@
+/*
+ * pairhmm_b200 -- PairHMM forward-algorithm engine for NVIDIA B200 (sm_100a).
+ *
+ * C ABI (plain pointers and sizes, int status codes, no exceptions across the
+ * boundary).  It is the drop-in for the forward path of asbschmidt/gpuPairHMM:
+ *
+ *   reference                                              replaced by
+ *   ------------------------------------------------------------------------------
+ *   BatchOfSequenceGroups (common.cuh:109-201)             pairhmm_batch_t
+ *   GpuPairHMMWorker ctor: ph2pr upload + streams
+ *     (gpuworker.cuh:401-416)                              pairhmm_engine_create
+ *   GpuPairHMMWorker dtor (gpuworker.cuh:418-428)          pairhmm_engine_destroy
+ *   GpuPairHMMWorker::processBatch_overlapped_float_
+ *     coalesced_smem (gpuworker.cuh:559-973): host batch
+ *     in, h_scores out                                     pairhmm_compute_host
+ *   MultiConfigGpuPairHMM::launchPairHMMSingleTileKernel
+ *     (gpuworker.cuh:220-274) and ::launchPairHMMMultiTile
+ *     Kernel (gpuworker.cuh:303-375): device arrays +
+ *     stream, scores written on the device                 pairhmm_compute_device
+ *   GpuPairHMMWorker::computeNumberOfDPCells
+ *     (gpuworker.cuh:495-520) and the GCUPS print
+ *     (gpuworker.cuh:426-427)                              pairhmm_get_stats
+ *   (no counterpart: the reference has no serving mode)    pairhmm_submit / _poll / _drain
+ *
+ * Scores: one float log10 likelihood per (read, haplotype) pair, written at
+ * slot  sum_{previous records} R*H + r*H + h  (gpuworker.cuh:1002-1021,
+ * pairhmm_kernels.cuh:1154).
+ *
+ * Threading: an engine is used by one host thread at a time (as the
+ * reference's worker is).  Different engines are independent.
+ */
+#ifndef PAIRHMM_B200_H
+#define PAIRHMM_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum pairhmm_status {
+    PAIRHMM_OK = 0,
+    PAIRHMM_ERR_INVALID_ARGUMENT = 1, /* null pointer, negative count, bad length */
+    PAIRHMM_ERR_CUDA = 2,             /* a CUDA runtime call failed; see pairhmm_last_error */
+    PAIRHMM_ERR_OUT_OF_MEMORY = 3,    /* device or pinned allocation failed */
+    PAIRHMM_ERR_BUDGET = 4,           /* serving: region larger than the device budget */
+    PAIRHMM_ERR_NOT_FOUND = 5,        /* serving: unknown ticket */
+    PAIRHMM_ERR_TIMEOUT = 6,          /* a bounded device wait gave up */
+    PAIRHMM_ERR_UNSUPPORTED = 7,      /* no sm_100 device, or feature not built */
+    PAIRHMM_ERR_BUSY = 8              /* serving: queue full, retry after draining */
+} pairhmm_status_t;
+
+/*
+ * One batch of records in the reference's structure-of-arrays layout
+ * (common.cuh:109-201).  Record g has reads_per_record[g] reads and
+ * haps_per_record[g] haplotypes; reads and haplotypes are numbered globally
+ * in record order.  Bases are ASCII (A, C, G, T; anything else counts as N,
+ * utility_kernels.cuh:6-23).  Qualities are Phred values, i.e. the file's
+ * ASCII minus 33 (file_parser_worker.cu:95); values above 127 are clamped to
+ * 127.  The byte arrays share one layout: read i occupies
+ * [read_offsets[i], read_offsets[i] + read_lengths[i]) in read_bases and in
+ * each quality array.  gcp_quals may be NULL: like the reference GPU path the
+ * engine uses a fixed gap-continuation probability of 0.1
+ * (pairhmm_kernels.cuh:1195-1196).
+ */
+typedef struct pairhmm_batch {
+    int64_t num_records;
+    const int32_t* reads_per_record; /* [num_records] */
+    const int32_t* haps_per_record;  /* [num_records] */
+    const uint8_t* read_bases;
+    const uint8_t* base_quals;
+    const uint8_t* ins_quals;
+    const uint8_t* del_quals;
+    const uint8_t* gcp_quals;    /* optional, ignored */
+    const int64_t* read_offsets; /* [num_reads] */
+    const int32_t* read_lengths; /* [num_reads], each >= 1 */
+    const uint8_t* hap_bases;
+    const int64_t* hap_offsets; /* [num_haps] */
+    const int32_t* hap_lengths; /* [num_haps], each >= 1 */
+} pairhmm_batch_t;
+
+/* Execution forms. */
+enum {
+    /* Persistent, length-bucketed, H-sorted work queue; tuned tile per bucket;
+     * CUDA-graph launched; FP64 rescue of FP32 underflows. */
+    PAIRHMM_MODE_ENGINE = 0,
+    /* One launch per read-length partition with the reference's generic tile
+     * table (tuningconfigs.hpp:33-57), no sorting, FP32 only.  Kept as the
+     * comparison baseline. */
+    PAIRHMM_MODE_PLAIN = 1
+};
+
+typedef struct pairhmm_options {
+    int32_t device;       /* CUDA ordinal, default 0 */
+    int32_t mode;         /* PAIRHMM_MODE_* */
+    int32_t fp64_rescue;  /* 1 (default): recompute FP32 underflows in FP64 */
+    int32_t use_graphs;   /* 1 (default): replay the per-batch launch sequence as a CUDA graph */
+    int64_t device_budget_bytes; /* serving admission budget; 0 = 40 GiB */
+} pairhmm_options_t;
+
+typedef struct pairhmm_stats {
+    int64_t pairs;           /* pairs in the last compute call */
+    int64_t cells;           /* sum L*H over those pairs */
+    int64_t rescued;         /* pairs recomputed in FP64 */
+    int64_t multi_tile_pairs;/* pairs whose read exceeded the largest single tile */
+    double device_ms;        /* device time of the last call (CUDA events, launch to scores) */
+    double total_ms;         /* host wall time of the last call */
+    double prep_ms;          /* of device_ms: packing and work-list construction */
+    double fp32_ms;          /* of device_ms: the FP32 wavefront launches */
+    double fp64_ms;          /* of device_ms: the FP64 pass */
+    int64_t launches;        /* kernels launched by the last call */
+    int64_t h2d_bytes;       /* host-to-device bytes copied by the last call */
+    int64_t d2h_bytes;       /* device-to-host bytes copied by the last call */
+} pairhmm_stats_t;
+
+typedef struct pairhmm_engine pairhmm_engine_t;
+
+/* Fill *opts with defaults. */
+void pairhmm_default_options(pairhmm_options_t* opts);
+
+pairhmm_status_t pairhmm_engine_create(const pairhmm_options_t* opts, pairhmm_engine_t** engine);
+pairhmm_status_t pairhmm_engine_destroy(pairhmm_engine_t* engine);
+
+/* Host arrays in, host scores out (float[sum R*H]).  Blocking. */
+pairhmm_status_t pairhmm_compute_host(pairhmm_engine_t* engine, const pairhmm_batch_t* batch,
+                                      float* scores);
+
+/* Device arrays in (every pointer in *batch is device memory), device scores
+ * out; work is ordered on `stream` (a cudaStream_t, NULL = legacy default)
+ * and the call returns without waiting.  max_read_length / max_hap_length
+ * bound the batch (0 = computed by the engine with one device-to-host read). */
+pairhmm_status_t pairhmm_compute_device(pairhmm_engine_t* engine, const pairhmm_batch_t* batch,
+                                        int32_t max_read_length, int32_t max_hap_length,
+                                        float* scores, void* stream);
+
+pairhmm_status_t pairhmm_get_stats(pairhmm_engine_t* engine, pairhmm_stats_t* stats);
+
+/* Serving (continuous batching).  submit copies the region to pinned staging
+ * and returns a ticket; regions submitted while others run are admitted into
+ * the device work queue as memory under the budget frees up.  poll reports
+ * completion without blocking; drain blocks (bounded by timeout_ms, <0 =
+ * forever) and copies the scores out, releasing the ticket. */
+pairhmm_status_t pairhmm_submit(pairhmm_engine_t* engine, const pairhmm_batch_t* region,
+                                uint64_t* ticket);
+pairhmm_status_t pairhmm_poll(pairhmm_engine_t* engine, uint64_t ticket, int32_t* done);
+pairhmm_status_t pairhmm_drain(pairhmm_engine_t* engine, uint64_t ticket, float* scores,
+                               int64_t num_scores, int32_t timeout_ms);
+
+/* Submit-to-completion time of a finished region (valid until it is drained). */
+pairhmm_status_t pairhmm_region_latency_ms(pairhmm_engine_t* engine, uint64_t ticket, double* ms);
+
+/*
+ * Tile table: reads of length in (max_len[i-1], max_len[i]] run with groups of
+ * group[i] lanes holding regs[i] read positions each (tile = group*regs), as
+ * one tile or, when multi_tile[i] != 0, as several.  This is the run-time form
+ * of the reference's compile-time tuning tables (tuningconfigs.hpp:33-269) and
+ * of its partition rule "first tile size >= read length"
+ * (utility_kernels.cuh:45-57).  Only compiled (group, regs) pairs are accepted;
+ * the last entry must be multi-tile.
+ */
+pairhmm_status_t pairhmm_set_tile_table(pairhmm_engine_t* engine, const int32_t* max_len, const int32_t* group,
+                                        const int32_t* regs, const int32_t* multi_tile, int32_t n);
+pairhmm_status_t pairhmm_get_tile_table(pairhmm_engine_t* engine, int32_t* max_len, int32_t* group,
+                                        int32_t* regs, int32_t* multi_tile, int32_t capacity, int32_t* n);
+
+/* Measurement utility (no counterpart in the reference): FP32 FMA throughput
+ * of `device` in TFLOP/s (2 FLOP per FMA), best of several launches of about
+ * `milliseconds` each.  Used as the roofline denominator. */
+pairhmm_status_t pairhmm_probe_fp32_peak(int32_t device, int32_t milliseconds, double* tflops);
+
+/*
+ * Record file format (README.md:41-61).  A parsed buffer owns its arrays; the
+ * view points into them (valid until pairhmm_records_free).
+ *   pairhmm_records_parse   FileParserWorker::parseNextSequenceGroup +
+ *                           convertGroupsToBatchInplace (file_parser_worker.cu:88-218):
+ *                           R/H header, 5 fields per read at k*(L+1), quality - 33,
+ *                           4 - len%4 bytes of 'N' padding (quality 'N'-33)
+ *   pairhmm_records_format  OutputWriterWorker::run (output_writer_worker.cu:107-135):
+ *                           "%d %d\n", then R lines of H "%.5f" joined by spaces.
+ *                           With buf == NULL (or capacity too small) only *len is set.
+ */
+typedef struct pairhmm_records pairhmm_records_t;
+pairhmm_status_t pairhmm_records_parse(const char* text, int64_t length, pairhmm_records_t** records);
+pairhmm_status_t pairhmm_records_view(const pairhmm_records_t* records, pairhmm_batch_t* view,
+                                      int64_t* num_pairs);
+pairhmm_status_t pairhmm_records_format(const pairhmm_records_t* records, const float* scores, char* buf,
+                                        int64_t capacity, int64_t* length);
+void pairhmm_records_free(pairhmm_records_t* records);
+
+const char* pairhmm_status_string(pairhmm_status_t status);
+/* Message of the last failing call on this engine (empty when none). */
+const char* pairhmm_last_error(const pairhmm_engine_t* engine);
+
+/* Number of pairs and DP cells of a host batch (gpuworker.cuh:495-520). */
+pairhmm_status_t pairhmm_batch_counts(const pairhmm_batch_t* batch, int64_t* pairs, int64_t* cells);
+
+/* Library version string. */
+const char* pairhmm_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PAIRHMM_B200_H */

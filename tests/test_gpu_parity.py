@@ -1,0 +1,215 @@
+"""CUDA path vs the oracle, through the C ABI, on seeded inputs.
+
+Tolerance: |gpu - oracle| <= 1e-5 * |oracle| + 1e-6 on log10 (conftest.RTOL/ATOL)."""
+import numpy as np
+import pytest
+
+import gpupairhmm_b200 as g
+import oracle
+from gpupairhmm_b200 import synth
+from conftest import ROOT, assert_log10_close
+
+pytestmark = pytest.mark.gpu
+GOLDEN = ROOT / "tests" / "golden"
+
+
+def test_readme_known_answers(engine):
+    recs = g.read_records_file(GOLDEN / "readme_example.in")
+    got = engine.compute(recs.batch)
+    lines = (GOLDEN / "readme_example.expected").read_text().split("\n")
+    want = np.array([float(x) for ln in lines[1:] if ln for x in ln.split()])
+    assert np.max(np.abs(got - want)) <= 1e-5
+    assert_log10_close(got, oracle.batch_log10(recs.batch), what="readme")
+
+
+@pytest.mark.parametrize("mode", ["engine", "plain"])
+def test_config0_matches_oracle(mode, engine, plain_engine):
+    e = engine if mode == "engine" else plain_engine
+    b = synth.config0(seed=0)
+    got = e.compute(b)
+    st = e.stats()
+    assert st.pairs == b.num_pairs and st.cells == b.cells()
+    assert_log10_close(got, oracle.batch_log10(b), what=f"cfg0 {mode}")
+
+
+def _record(rng, L, H, n_reads=2, n_haps=2, letters="ACGT", bq=(10, 41), idq=(30, 46), related=True):
+    reads, haps = [], []
+    for _ in range(n_haps):
+        haps.append(bytes(rng.choice(list(letters.encode()), size=H).astype(np.uint8)))
+    for i in range(n_reads):
+        if related and H >= L and i % 2 == 0:
+            s = int(rng.integers(0, H - L + 1))
+            r = bytearray(haps[0][s:s + L])
+        else:
+            r = bytearray(rng.choice(list(letters.encode()), size=L).astype(np.uint8))
+        q = [rng.integers(*bq, size=L), rng.integers(*idq, size=L), rng.integers(*idq, size=L)]
+        reads.append((bytes(r), *[bytes(x.astype(np.uint8)) for x in q], bytes([10] * L)))
+    from oracle.formats import Record
+    return Record(reads=reads, haps=haps)
+
+
+def _soa(records):
+    from oracle.formats import to_soa
+    s = to_soa(records)
+    return g.Batch(s.reads_per_record, s.haps_per_record, s.read_bases, s.base_quals, s.ins_quals, s.del_quals,
+                   s.read_offsets, s.read_lengths, s.hap_bases, s.hap_offsets, s.hap_lengths, s.gcp_quals)
+
+
+def test_length_sweep_across_tile_boundaries(engine, plain_engine):
+    rng = np.random.default_rng(5)
+    lens = list(range(1, 41)) + [47, 48, 49, 63, 64, 65, 79, 80, 81, 95, 96, 97, 111, 112, 113, 127, 128, 129,
+                                 159, 160, 161, 191, 192, 193, 223, 224, 225, 255, 256, 257, 319, 320, 321,
+                                 383, 384, 385, 447, 448, 449, 511, 512, 513, 639, 640, 641, 767, 768, 769,
+                                 895, 896, 897, 1023, 1024, 1025]
+    recs = []
+    for i, L in enumerate(lens):
+        H = int(rng.choice([1, 2, 3, 5, 16, 17, L, L + 7, 2 * L + 3]))
+        recs.append(_record(rng, L, max(H, 1), n_reads=2, n_haps=1 + i % 3))
+    b = _soa(recs)
+    want = oracle.batch_log10(b)
+    assert_log10_close(engine.compute(b), want, what="sweep engine")
+    assert_log10_close(plain_engine.compute(b), want, what="sweep plain")
+
+
+def test_haplotype_length_sweep(engine):
+    rng = np.random.default_rng(6)
+    recs = [_record(rng, 100, H, n_reads=3, n_haps=2) for H in
+            list(range(1, 34)) + [63, 64, 65, 127, 128, 129, 1000, 4097, 5000]]
+    b = _soa(recs)
+    assert_log10_close(engine.compute(b), oracle.batch_log10(b), what="hap sweep")
+
+
+def test_n_lowercase_and_odd_letters(engine):
+    rng = np.random.default_rng(8)
+    recs = [_record(rng, L, H, letters="ACGTNacgtX") for L, H in [(7, 9), (64, 80), (150, 300), (250, 260)]]
+    b = _soa(recs)
+    assert_log10_close(engine.compute(b), oracle.batch_log10(b), what="letters")
+
+
+def test_quality_extremes_and_degenerate_alpha(engine):
+    """Qualities 0..93 and ins/del qualities low enough that 1-(delta+sigma) is
+    near or below zero (the FP32 kernel hands those pairs to the FP64 pass)."""
+    rng = np.random.default_rng(9)
+    recs = []
+    for bq, idq in [((0, 94), (30, 46)), ((10, 41), (0, 4)), ((10, 41), (3, 4)), ((0, 3), (0, 94))]:
+        for L, H in [(20, 40), (100, 150), (300, 400)]:
+            recs.append(_record(rng, L, H, bq=bq, idq=idq))
+    b = _soa(recs)
+    want = oracle.batch_log10(b)
+    got = engine.compute(b)
+    fin = np.isfinite(want)
+    assert np.array_equal(fin, np.isfinite(got))
+    assert_log10_close(got[fin], want[fin], what="quality extremes")
+
+
+def test_fp64_rescue_of_underflowing_pairs(engine):
+    b = synth.config2(seed=12, regions=4)
+    want = oracle.batch_log10(b)
+    got = engine.compute(b)
+    st = engine.stats()
+    under = want < -67.0
+    assert under.sum() > 0.3 * len(want)
+    assert st.rescued >= under.sum()
+    assert_log10_close(got, want, what="cfg2 with rescue")
+
+
+def test_rescue_disabled_keeps_fp32_results():
+    e = g.Engine(fp64_rescue=False)
+    b = synth.config2(seed=12, regions=2)
+    want = oracle.batch_log10(b)
+    got = e.compute(b)
+    ok = want > -60.0
+    assert_log10_close(got[ok], want[ok], what="cfg2 fp32 part")
+    e.close()
+
+
+def test_multi_tile_long_reads(engine, plain_engine):
+    b = synth.config3(seed=13, regions=2)
+    want = oracle.batch_log10(b)
+    got = engine.compute(b)
+    assert engine.stats().multi_tile_pairs > 0
+    fin = want > -67
+    assert_log10_close(got, want, what="cfg3 engine")
+    assert_log10_close(plain_engine.compute(b)[fin], want[fin], what="cfg3 plain")
+
+
+def test_very_long_read_many_tiles(engine):
+    rng = np.random.default_rng(14)
+    recs = [_record(rng, 4500, 5200, n_reads=2, n_haps=1), _record(rng, 2049, 300, n_reads=1, n_haps=2)]
+    b = _soa(recs)
+    assert_log10_close(engine.compute(b), oracle.batch_log10(b), what="long read")
+
+
+def test_empty_and_ragged_records(engine):
+    rng = np.random.default_rng(15)
+    from oracle.formats import Record
+    recs = [_record(rng, 30, 40, n_reads=3, n_haps=2), Record(reads=[], haps=[b"ACGT"]),
+            _record(rng, 5, 7, n_reads=1, n_haps=1), Record(reads=_record(rng, 9, 9).reads, haps=[]),
+            _record(rng, 200, 90, n_reads=7, n_haps=5)]
+    b = _soa(recs)
+    got = engine.compute(b)
+    assert len(got) == b.num_pairs
+    assert_log10_close(got, oracle.batch_log10(b), what="ragged")
+    # a batch without pairs
+    e = _soa([Record(reads=[], haps=[b"AC"])])
+    assert len(engine.compute(e)) == 0
+
+
+def test_results_do_not_depend_on_batch_composition(engine):
+    """Each pair's result is computed independently: alone, in a bigger batch
+    and after shuffling the records it is bitwise the same."""
+    b = synth.config1(seed=16, regions=40)
+    full = engine.compute(b)
+    po = np.r_[0, np.cumsum(b.reads_per_record.astype(np.int64) * b.haps_per_record)]
+    for first, last in [(0, 1), (5, 9), (39, 40)]:
+        part = engine.compute(b.select_records(first, last))
+        np.testing.assert_array_equal(part, full[po[first]:po[last]])
+
+
+def test_graphs_and_direct_launches_agree():
+    b = synth.config1(seed=17, regions=20)
+    a = g.Engine(use_graphs=True).compute(b)
+    c = g.Engine(use_graphs=False).compute(b)
+    np.testing.assert_array_equal(a, c)
+
+
+def test_repeat_calls_are_deterministic(engine):
+    b = synth.config1(seed=18, regions=25)
+    x = engine.compute(b)
+    y = engine.compute(synth.config0(seed=3))
+    z = engine.compute(b)
+    np.testing.assert_array_equal(x, z)
+    assert len(y) == 8192
+
+
+def test_device_api_matches_host_api(engine):
+    import torch
+    b = synth.config1(seed=19, regions=15)
+    host = engine.compute(b)
+    d = b.to_device()
+    scores = torch.empty(b.num_pairs, dtype=torch.float32, device="cuda")
+    s = torch.cuda.Stream()
+    engine.compute_device(d, scores, stream=s)
+    s.synchronize()
+    np.testing.assert_array_equal(scores.cpu().numpy(), host)
+
+
+def test_pinned_host_inputs(engine):
+    b = synth.config0(seed=4, records=8)
+    np.testing.assert_array_equal(engine.compute(b.pin()), engine.compute(b))
+
+
+def test_tile_table_round_trip_and_validation():
+    e = g.Engine()
+    t = e.tile_table()
+    assert t[-1][3]
+    b = synth.config1(seed=20, regions=10)
+    base = e.compute(b)
+    # a coarser table (different tiles) gives the same results within tolerance
+    e.set_tile_table([(128, 8, 16, False), (256, 16, 16, False), (512, 32, 16, False), (1 << 30, 32, 32, True)])
+    assert_log10_close(e.compute(b), base, what="alt table")
+    with pytest.raises(g.PairHMMError):
+        e.set_tile_table([(128, 4, 8, False), (1 << 30, 32, 32, True)])  # 128 > 4*8
+    with pytest.raises(g.PairHMMError):
+        e.set_tile_table([(128, 4, 32, False)])  # last rule must be multi-tile
+    e.close()
