@@ -50,8 +50,8 @@ struct DevView {
     const int64_t* hap_start;  // in bytes, multiple of 16
     const int32_t* hap_len;
     float* scores;
-    Task* rescue;               // FP32 results below kRescueThreshold are appended here
-    unsigned long long* rescue_count;
+    Task* rescue[3];            // flagged pairs by read-length class (fp64_class)
+    unsigned long long* rescue_count;  // [3]
     int rescue_enabled;
     const float* ph2pr;         // 128 floats in global memory
 };
@@ -62,5 +62,13 @@ __device__ __forceinline__ uint32_t code_of(uint8_t c) {
 }
 
 __device__ __forceinline__ int min_i(int a, int b) { return a < b ? a : b; }
+
+// FP64 pass classes: reads up to 64 and 128 positions run 4 and 2 pairs per
+// warp (single tile); longer reads one pair per warp, multi-tile.
+constexpr int kFp64ClassMax0 = 64;
+constexpr int kFp64ClassMax1 = 128;
+__host__ __device__ __forceinline__ int fp64_class(int L) {
+    return L <= kFp64ClassMax0 ? 0 : (L <= kFp64ClassMax1 ? 1 : 2);
+}
 
 }  // namespace phmm

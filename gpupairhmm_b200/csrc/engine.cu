@@ -87,7 +87,8 @@ Engine::Engine(const pairhmm_options_t& opts) : opts_(opts) {
 
 Engine::~Engine() {
     if (ready_) cudaSetDevice(opts_.device);
-    if (graph_exec_) cudaGraphExecDestroy(graph_exec_);
+    for (cudaGraphExec_t& g : graph_exec_)
+        if (g) cudaGraphExecDestroy(g);
     DevBuf* bufs[] = {&ph2pr_, &rules_maxlen_, &rules_rank_, &per_task_, &config_, &in_read_bases_, &in_bq_,
                       &in_iq_, &in_dq_, &in_read_off_, &in_read_len_, &in_hap_bases_, &in_hap_off_, &in_hap_len_,
                       &read_record_, &read_local_, &rec_haps_, &rec_hap_base_, &rec_pair_base_, &read_start_,
@@ -137,15 +138,16 @@ pairhmm_status_t Engine::init() {
     // dynamic shared memory opt-in for every kernel on this device
     for (const ConfigInfo& c : fp32_configs())
         PHMM_CUDA(cudaFuncSetAttribute(c.kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c.smem_bytes));
-    PHMM_CUDA(cudaFuncSetAttribute(fp64_kernel(), cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   (int)fp64_smem_bytes()));
+    for (int c = 0; c < 3; ++c)
+        PHMM_CUDA(cudaFuncSetAttribute(fp64_kernel(c), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)fp64_smem_bytes(c)));
 
     // probability table p(q) = float(10^(-q/10)) (gpuworker.cuh:473-486)
     float table[128];
     for (int i = 0; i < 128; ++i) table[i] = (float)std::pow(10.0, (-i) / 10.0);
     PHMM_CUDA(ph2pr_.ensure(sizeof(table)));
     PHMM_CUDA(cudaMemcpy(ph2pr_.ptr, table, sizeof(table), cudaMemcpyHostToDevice));
-    PHMM_CUDA(counters_.ensure(sizeof(unsigned long long) * (kMaxBuckets + 4)));
+    PHMM_CUDA(counters_.ensure(sizeof(unsigned long long) * (kMaxBuckets + 8)));
     PHMM_CUDA(sched_.ensure(sizeof(Schedule)));
     ready_ = true;
     return upload_rules();
@@ -163,9 +165,9 @@ pairhmm_status_t Engine::set_tile_table(const std::vector<TileRule>& rules) {
     }
     if (!rules.back().multi_tile) return fail(PAIRHMM_ERR_INVALID_ARGUMENT, "last rule must be multi-tile");
     rules_ = rules;
-    if (graph_exec_) {
-        cudaGraphExecDestroy(graph_exec_);
-        graph_exec_ = nullptr;
+    for (cudaGraphExec_t& g : graph_exec_) {
+        if (g) cudaGraphExecDestroy(g);
+        g = nullptr;
     }
     return ready_ ? upload_rules() : PAIRHMM_OK;
 }
@@ -250,6 +252,7 @@ pairhmm_status_t Engine::build_index(const pairhmm_batch_t& b, const std::vector
         const int bk = bucket_of_host(L, rules);
         const int64_t H = x.rec_haps[x.read_record[i]];
         x.bucket_pairs[bk] += H;
+        x.class_pairs[fp64_class(L)] += H;
         if (rules[bk].multi_tile) x.multi_tile_pairs += H;
     }
     for (int64_t h = 0; h < x.num_haps; ++h) {
@@ -307,7 +310,7 @@ pairhmm_status_t Engine::ensure_buffers(const BatchIndex& x, bool host_inputs) {
     PHMM_CUDA(hist_.ensure(4 * nbins));
     PHMM_CUDA(cursor_.ensure(8 * nbins));
     PHMM_CUDA(items_.ensure(sizeof(Task) * np));
-    PHMM_CUDA(rescue_.ensure(sizeof(Task) * np));
+    PHMM_CUDA(rescue_.ensure(sizeof(Task) * np));  // class lists laid out back to back
     return PAIRHMM_OK;
 }
 
@@ -360,7 +363,7 @@ int Engine::persistent_grid(const void* kernel, size_t smem) const {
 }
 
 pairhmm_status_t Engine::enqueue_pipeline(const pairhmm_batch_t& in, const BatchIndex& x, const Plan& plan,
-                                          float* d_scores, cudaStream_t s) {
+                                          float* d_scores, cudaStream_t s, int stage) {
     const int nb = (int)rules_.size();
     const bool plain = opts_.mode == PAIRHMM_MODE_PLAIN;
     const int prep_grid = 4 * num_sms_;
@@ -386,10 +389,12 @@ pairhmm_status_t Engine::enqueue_pipeline(const pairhmm_batch_t& in, const Batch
     pa.num_haps = x.num_haps;
     pa.read_pack = read_pack_.as<uint32_t>();
     pa.hap_code = hap_code_.as<uint8_t>();
+    if (stage == 0) {
     launches_ = 0;
     PHMM_CUDA(launch_pack(pa, prep_grid, s));
     launches_ += 2;
     PHMM_CUDA(cudaMemsetAsync(hap_code_.as<uint8_t>() + x.code_bytes, 4, kHapSlack, s));
+    }
 
     BinArgs ba{};
     ba.read_lengths = in.read_lengths;
@@ -407,10 +412,12 @@ pairhmm_status_t Engine::enqueue_pipeline(const pairhmm_batch_t& in, const Batch
     ba.hist = hist_.as<unsigned int>();
     ba.cursor = cursor_.as<unsigned long long>();
     ba.items = items_.as<Task>();
+    if (stage == 0) {
     PHMM_CUDA(launch_binning(ba, prep_grid, s, per_task_.as<int>(), config_.as<int>(), sched_.as<Schedule>(), nb));
     launches_ += 4;
-    PHMM_CUDA(cudaMemsetAsync(counters_.ptr, 0, sizeof(unsigned long long) * (kMaxBuckets + 4), s));
-    PHMM_CUDA(cudaEventRecord(ev_prep_, s));
+    PHMM_CUDA(cudaMemsetAsync(counters_.ptr, 0, sizeof(unsigned long long) * (kMaxBuckets + 8), s));
+    return PAIRHMM_OK;
+    }
 
     unsigned long long* counters = counters_.as<unsigned long long>();
     DevView v{};
@@ -421,11 +428,18 @@ pairhmm_status_t Engine::enqueue_pipeline(const pairhmm_batch_t& in, const Batch
     v.hap_start = pa.hap_start;
     v.hap_len = in.hap_lengths;
     v.scores = d_scores;
-    v.rescue = rescue_.as<Task>();
+    {
+        int64_t off = 0;
+        for (int c = 0; c < 3; ++c) {
+            v.rescue[c] = rescue_.as<Task>() + off;
+            off += x.class_pairs[c];
+        }
+    }
     v.rescue_count = counters + kMaxBuckets;
     v.rescue_enabled = (!plain && opts_.fp64_rescue) ? 1 : 0;
     v.ph2pr = ph2pr_.as<float>();
 
+    if (stage == 1) {
     for (int rank = 0; rank < nb; ++rank) {
         const int b = plain ? rank : nb - 1 - rank;
         if (x.bucket_pairs[b] == 0) continue;
@@ -444,17 +458,20 @@ pairhmm_status_t Engine::enqueue_pipeline(const pairhmm_batch_t& in, const Batch
         PHMM_CUDA(c->launch(la));
         ++launches_;
     }
-    PHMM_CUDA(cudaEventRecord(ev_fp32_, s));
-    // FP64 pass over flagged pairs (FP32 underflow, or degenerate alpha)
-    {
+    return PAIRHMM_OK;
+    }
+    // stage 2: FP64 pass over flagged pairs (FP32 underflow, or degenerate alpha)
+    for (int c = 0; c < 3; ++c) {
+        if (x.class_pairs[c] == 0) continue;
         Fp64LaunchArgs fa{};
         fa.view = v;
-        fa.items = rescue_.as<Task>();
-        fa.count = counters + kMaxBuckets;
-        fa.counter = counters + kMaxBuckets + 1;
+        fa.cls = c;
+        fa.items = v.rescue[c];
+        fa.count = counters + kMaxBuckets + c;
+        fa.counter = counters + kMaxBuckets + 3 + c;
         fa.scratch = scratch_.ptr;
         fa.rows = plan.rows;
-        fa.grid = plan.fp64_grid;
+        fa.grid = plan.fp64_grid[c];
         fa.stream = s;
         PHMM_CUDA(launch_fp64_rescue(fa));
         ++launches_;
@@ -487,12 +504,17 @@ Engine::Plan Engine::make_plan(const BatchIndex& x) const {
         // the plain form runs one task per warp; a grid capped by scratch loops on the counter
         p.persistent[b] = (!plain || grid < need_blocks) ? 1 : 0;
     }
-    {
-        const int64_t per_warp = (int64_t)fp64_scratch_bytes_per_row() * p.rows;
-        int64_t grid = persistent_grid(fp64_kernel(), fp64_smem_bytes());
-        grid = std::min<int64_t>(grid, std::max<int64_t>(1, kScratchBudget / (per_warp * kWarpsPerBlock)));
-        p.fp64_grid = (int)grid;
-        scratch = std::max(scratch, grid * kWarpsPerBlock * per_warp);
+    for (int c = 0; c < 3; ++c) {
+        int64_t grid = persistent_grid(fp64_kernel(c), fp64_smem_bytes(c));
+        const int64_t per_warp = (int64_t)fp64_scratch_bytes_per_row(c) * p.rows;
+        if (per_warp > 0) {
+            grid = std::min<int64_t>(grid, std::max<int64_t>(1, kScratchBudget / (per_warp * kWarpsPerBlock)));
+            scratch = std::max(scratch, grid * kWarpsPerBlock * per_warp);
+        }
+        // no more warps than flagged pairs could need
+        const int64_t need = (x.class_pairs[c] + fp64_per_warp(c) - 1) / fp64_per_warp(c);
+        grid = std::min<int64_t>(grid, std::max<int64_t>(1, (need + kWarpsPerBlock - 1) / kWarpsPerBlock));
+        p.fp64_grid[c] = (int)grid;
     }
     p.scratch_bytes = (size_t)std::max<int64_t>(scratch, 256);
     return p;
@@ -504,37 +526,45 @@ pairhmm_status_t Engine::run_pipeline(const pairhmm_batch_t& in, const BatchInde
     // every buffer the launches reference exists before capture starts
     const Plan plan = make_plan(x);
     PHMM_CUDA(scratch_.ensure(plan.scratch_bytes));
-    if (!opts_.use_graphs) return enqueue_pipeline(in, x, plan, d_scores, s);
-
-    cudaGraph_t graph = nullptr;
-    PHMM_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
-    pairhmm_status_t st = enqueue_pipeline(in, x, plan, d_scores, s);
-    cudaError_t ce = cudaStreamEndCapture(s, &graph);
-    if (st != PAIRHMM_OK) {
-        if (graph) cudaGraphDestroy(graph);
-        return st;
-    }
-    if (ce != cudaSuccess) return cuda_fail(ce, "cudaStreamEndCapture");
-    bool updated = false;
-    if (graph_exec_) {
-        cudaGraphExecUpdateResultInfo info{};
-        if (cudaGraphExecUpdate(graph_exec_, graph, &info) == cudaSuccess) updated = true;
-        else {
-            cudaGetLastError();
-            cudaGraphExecDestroy(graph_exec_);
-            graph_exec_ = nullptr;
-        }
-    }
-    if (!updated) {
-        ce = cudaGraphInstantiate(&graph_exec_, graph, 0);
-        if (ce != cudaSuccess) {
+    cudaEvent_t marks[3] = {ev_prep_, ev_fp32_, ev1_};
+    for (int stage = 0; stage < 3; ++stage) {
+        if (!opts_.use_graphs) {
+            pairhmm_status_t st = enqueue_pipeline(in, x, plan, d_scores, s, stage);
+            if (st != PAIRHMM_OK) return st;
+        } else {
+            cudaGraph_t graph = nullptr;
+            PHMM_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+            pairhmm_status_t st = enqueue_pipeline(in, x, plan, d_scores, s, stage);
+            cudaError_t ce = cudaStreamEndCapture(s, &graph);
+            if (st != PAIRHMM_OK) {
+                if (graph) cudaGraphDestroy(graph);
+                return st;
+            }
+            if (ce != cudaSuccess) return cuda_fail(ce, "cudaStreamEndCapture");
+            cudaGraphExec_t& exec = graph_exec_[stage];
+            bool updated = false;
+            if (exec) {
+                cudaGraphExecUpdateResultInfo info{};
+                if (cudaGraphExecUpdate(exec, graph, &info) == cudaSuccess) updated = true;
+                else {
+                    cudaGetLastError();
+                    cudaGraphExecDestroy(exec);
+                    exec = nullptr;
+                }
+            }
+            if (!updated) {
+                ce = cudaGraphInstantiate(&exec, graph, 0);
+                if (ce != cudaSuccess) {
+                    cudaGraphDestroy(graph);
+                    exec = nullptr;
+                    return cuda_fail(ce, "cudaGraphInstantiate");
+                }
+            }
             cudaGraphDestroy(graph);
-            graph_exec_ = nullptr;
-            return cuda_fail(ce, "cudaGraphInstantiate");
+            PHMM_CUDA(cudaGraphLaunch(exec, s));
         }
+        PHMM_CUDA(cudaEventRecord(marks[stage], s));
     }
-    cudaGraphDestroy(graph);
-    PHMM_CUDA(cudaGraphLaunch(graph_exec_, s));
     return PAIRHMM_OK;
 }
 
@@ -588,10 +618,9 @@ pairhmm_status_t Engine::compute_host(const pairhmm_batch_t& b, float* scores) {
 
     PHMM_CUDA(cudaEventRecord(ev0_, s));
     if ((st = run_pipeline(dev, x, scores_.as<float>(), s)) != PAIRHMM_OK) return st;
-    PHMM_CUDA(cudaEventRecord(ev1_, s));
     PHMM_CUDA(cudaMemcpyAsync(scores, scores_.ptr, 4 * x.num_pairs, cudaMemcpyDeviceToHost, s));
-    unsigned long long rescued = 0;
-    PHMM_CUDA(cudaMemcpyAsync(&rescued, counters_.as<unsigned long long>() + kMaxBuckets, sizeof(rescued),
+    unsigned long long rescued3[3] = {0, 0, 0};
+    PHMM_CUDA(cudaMemcpyAsync(rescued3, counters_.as<unsigned long long>() + kMaxBuckets, sizeof(rescued3),
                               cudaMemcpyDeviceToHost, s));
     PHMM_CUDA(cudaStreamSynchronize(s));
     float ms = 0.f, a = 0.f, b2 = 0.f, c = 0.f;
@@ -605,8 +634,8 @@ pairhmm_status_t Engine::compute_host(const pairhmm_batch_t& b, float* scores) {
     stats_.fp64_ms = c;
     stats_.launches = launches_;
     stats_.h2d_bytes = 4 * rn + hn + 12 * x.num_reads + 12 * x.num_haps + index_bytes(x);
-    stats_.d2h_bytes = 4 * x.num_pairs + (int64_t)sizeof(rescued);
-    stats_.rescued = (int64_t)rescued;
+    stats_.d2h_bytes = 4 * x.num_pairs + (int64_t)sizeof(rescued3);
+    stats_.rescued = (int64_t)(rescued3[0] + rescued3[1] + rescued3[2]);
     stats_.total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     return PAIRHMM_OK;
 }
@@ -654,7 +683,6 @@ pairhmm_status_t Engine::compute_device(const pairhmm_batch_t& b, int32_t, int32
     if ((st = upload_index(x, s)) != PAIRHMM_OK) return st;
     PHMM_CUDA(cudaEventRecord(ev0_, s));
     if ((st = run_pipeline(b, x, scores, s)) != PAIRHMM_OK) return st;
-    PHMM_CUDA(cudaEventRecord(ev1_, s));
     PHMM_CUDA(cudaStreamWaitEvent(stream, ev1_, 0));
     stats_.total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     stats_.device_ms = -1.0;

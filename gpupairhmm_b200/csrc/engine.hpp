@@ -31,6 +31,7 @@ struct BatchIndex {
     std::vector<int32_t> read_record, read_local, rec_haps;
     std::vector<int64_t> rec_hap_base, rec_pair_base, read_start, hap_start;
     std::vector<int64_t> bucket_pairs;              // by bucket index
+    int64_t class_pairs[3] = {0, 0, 0};             // by FP64 length class (fp64_class)
     int64_t multi_tile_pairs = 0;
 };
 
@@ -77,12 +78,13 @@ private:
         int64_t rows = 0;                 // border rows per buffer
         std::vector<int> grid;            // by bucket
         std::vector<int> persistent;      // by bucket
-        int fp64_grid = 0;
+        int fp64_grid[3] = {0, 0, 0};   // by FP64 length class
         size_t scratch_bytes = 0;
     };
     Plan make_plan(const BatchIndex& idx) const;
+    // stage 0: packing + work list, 1: FP32 launches, 2: FP64 pass
     pairhmm_status_t enqueue_pipeline(const pairhmm_batch_t& dev_in, const BatchIndex& idx, const Plan& plan,
-                                      float* d_scores, cudaStream_t s);
+                                      float* d_scores, cudaStream_t s, int stage);
     pairhmm_status_t ensure_buffers(const BatchIndex& idx, bool host_inputs);
     pairhmm_status_t upload_index(const BatchIndex& idx, cudaStream_t s);
     int persistent_grid(const void* kernel, size_t smem) const;
@@ -96,7 +98,7 @@ private:
     cudaStream_t stream_ = nullptr;
     cudaEvent_t ev0_ = nullptr, ev1_ = nullptr, ev_prep_ = nullptr, ev_fp32_ = nullptr;
     int64_t launches_ = 0;
-    cudaGraphExec_t graph_exec_ = nullptr;
+    cudaGraphExec_t graph_exec_[3] = {nullptr, nullptr, nullptr};  // prep, FP32, FP64
     pairhmm_stats_t stats_{};
     std::string last_error_;
 

@@ -12,7 +12,7 @@
 
 namespace phmm {
 
-constexpr int kBlockThreads = 128;  // 4 warps per CTA
+constexpr int kBlockThreads = 64;  // 2 warps per CTA: register-bound configs reach 10 warps/SM
 constexpr int kWarpsPerBlock = kBlockThreads / 32;
 
 struct Fp32LaunchArgs {
@@ -30,10 +30,11 @@ struct Fp32LaunchArgs {
 
 struct Fp64LaunchArgs {
     DevView view;
-    const Task* items;               // rescue list
+    int cls;                         // length class (fp64_class)
+    const Task* items;               // that class's rescue list
     const unsigned long long* count; // number of items (device)
     unsigned long long* counter;     // task counter
-    void* scratch;
+    void* scratch;                   // border storage (class 2 only)
     int64_t rows;
     int grid;
     cudaStream_t stream;
@@ -55,12 +56,13 @@ struct ConfigInfo {
 const std::vector<ConfigInfo>& fp32_configs();
 const ConfigInfo* find_fp32_config(int G, int R, bool multi_tile);
 
-// FP64 rescue kernel (G = 32, R = 8, multi-tile capable).
+// FP64 pass, one kernel per length class: (G, R) = (8, 8), (16, 8) single
+// tile and (32, 8) multi-tile.
 cudaError_t launch_fp64_rescue(const Fp64LaunchArgs& a);
-size_t fp64_smem_bytes();
-size_t fp64_scratch_bytes_per_row();  // per warp, per border row
-const void* fp64_kernel();
-int fp64_tile();
+size_t fp64_smem_bytes(int cls);
+size_t fp64_scratch_bytes_per_row(int cls);  // per warp, per border row
+const void* fp64_kernel(int cls);
+int fp64_per_warp(int cls);
 
 // Preparation kernels.
 cudaError_t launch_pack(const PrepArgs& a, int grid, cudaStream_t s);

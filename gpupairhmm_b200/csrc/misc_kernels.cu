@@ -33,10 +33,13 @@ const ConfigInfo* find_fp32_config(int G, int R, bool multi_tile) {
     return nullptr;
 }
 
-// ---------------------------------------------------------------- FP64 rescue
-constexpr int kFp64R = 8;
-using W64 = Fp64Wavefront<kFp64R>;
+// ---------------------------------------------------------------- FP64 pass
+using W64c0 = Fp64Wavefront<8, 8, false>;
+using W64c1 = Fp64Wavefront<16, 8, false>;
+using W64c2 = Fp64Wavefront<32, 8, true>;
+static_assert(W64c0::T == kFp64ClassMax0 && W64c1::T == kFp64ClassMax1, "class bounds follow the tiles");
 
+template <class W>
 __global__ void __launch_bounds__(kBlockThreads)
 fp64_rescue_kernel(DevView v, const Task* __restrict__ items, const unsigned long long* count,
                    unsigned long long* counter, Border64* scratch, int64_t rows) {
@@ -44,34 +47,54 @@ fp64_rescue_kernel(DevView v, const Task* __restrict__ items, const unsigned lon
     float* ph = reinterpret_cast<float*>(smem64);  // 128 floats = 32 double2
     const int warp = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
-    double2* wtab = smem64 + 32 + warp * W64::kTableDouble2;
-    Border64* ring = reinterpret_cast<Border64*>(smem64 + 32 + kWarpsPerBlock * W64::kTableDouble2) +
-                     warp * W64::kRing;
+    double2* wtab = smem64 + 32 + warp * W::kTableDouble2;
+    Border64* ring = reinterpret_cast<Border64*>(smem64 + 32 + kWarpsPerBlock * W::kTableDouble2) +
+                     warp * W::kRing;
     for (int i = threadIdx.x; i < 128; i += blockDim.x) ph[i] = v.ph2pr[i];
     __syncthreads();
     const unsigned long long n = *count;
+    const unsigned long long ntasks = (n + W::NG - 1) / W::NG;
     const long long gwarp = (long long)blockIdx.x * kWarpsPerBlock + warp;
-    Border64* wscratch = scratch + gwarp * 2 * rows;
+    Border64* wscratch = scratch ? scratch + gwarp * 2 * rows : nullptr;
     while (true) {
         unsigned long long x = 0;
         if (lane == 0) x = atomicAdd(counter, 1ull);
         x = __shfl_sync(kFullMask, x, 0);
-        if (x >= n) break;
-        W64::run(v, items[x], ph, wtab, ring, wscratch, rows);
+        if (x >= ntasks) break;
+        const unsigned long long first = x * W::NG;
+        const int ntask = (int)((n - first) < (unsigned long long)W::NG ? (n - first) : W::NG);
+        W::run(v, items + first, ntask, ph, wtab, ring, wscratch, rows);
     }
 }
 
-size_t fp64_smem_bytes() {
-    return (32 + (size_t)kWarpsPerBlock * W64::kTableDouble2) * sizeof(double2) +
-           (size_t)kWarpsPerBlock * W64::kRing * sizeof(Border64);
+template <class W>
+size_t fp64_smem_for() {
+    return (32 + (size_t)kWarpsPerBlock * W::kTableDouble2) * sizeof(double2) +
+           (size_t)kWarpsPerBlock * W::kRing * sizeof(Border64);
 }
-size_t fp64_scratch_bytes_per_row() { return 2 * sizeof(Border64); }
-const void* fp64_kernel() { return reinterpret_cast<const void*>(&fp64_rescue_kernel); }
-int fp64_tile() { return W64::T; }
+
+size_t fp64_smem_bytes(int cls) {
+    return cls == 0 ? fp64_smem_for<W64c0>() : cls == 1 ? fp64_smem_for<W64c1>() : fp64_smem_for<W64c2>();
+}
+size_t fp64_scratch_bytes_per_row(int cls) { return cls == 2 ? 2 * sizeof(Border64) : 0; }
+const void* fp64_kernel(int cls) {
+    return cls == 0 ? reinterpret_cast<const void*>(&fp64_rescue_kernel<W64c0>)
+         : cls == 1 ? reinterpret_cast<const void*>(&fp64_rescue_kernel<W64c1>)
+                    : reinterpret_cast<const void*>(&fp64_rescue_kernel<W64c2>);
+}
+int fp64_per_warp(int cls) { return cls == 0 ? W64c0::NG : cls == 1 ? W64c1::NG : W64c2::NG; }
 
 cudaError_t launch_fp64_rescue(const Fp64LaunchArgs& a) {
-    fp64_rescue_kernel<<<a.grid, kBlockThreads, fp64_smem_bytes(), a.stream>>>(
-        a.view, a.items, a.count, a.counter, static_cast<Border64*>(a.scratch), a.rows);
+    Border64* scr = static_cast<Border64*>(a.scratch);
+    if (a.cls == 0)
+        fp64_rescue_kernel<W64c0><<<a.grid, kBlockThreads, fp64_smem_bytes(0), a.stream>>>(
+            a.view, a.items, a.count, a.counter, nullptr, a.rows);
+    else if (a.cls == 1)
+        fp64_rescue_kernel<W64c1><<<a.grid, kBlockThreads, fp64_smem_bytes(1), a.stream>>>(
+            a.view, a.items, a.count, a.counter, nullptr, a.rows);
+    else
+        fp64_rescue_kernel<W64c2><<<a.grid, kBlockThreads, fp64_smem_bytes(2), a.stream>>>(
+            a.view, a.items, a.count, a.counter, scr, a.rows);
     return cudaGetLastError();
 }
 

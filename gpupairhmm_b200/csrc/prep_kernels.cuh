@@ -117,6 +117,19 @@ __device__ __forceinline__ int bin_of(const BinArgs& a, int L, int H) {
 }
 
 #ifdef PHMM_PREP_KERNELS_IMPL
+// warp-aggregated increment: lanes that hit the same counter share one atomic
+template <class T>
+__device__ __forceinline__ T aggregated_add(T* counter, unsigned key) {
+    const unsigned active = __activemask();
+    const unsigned peers = __match_any_sync(active, key);
+    const int leader = __ffs(peers) - 1;
+    const int lane = threadIdx.x & 31;
+    T base = 0;
+    if (lane == leader) base = atomicAdd(counter, (T)__popc(peers));
+    base = __shfl_sync(peers, base, leader);
+    return base + (T)__popc(peers & ((1u << lane) - 1u));
+}
+
 // thread per read: histogram of (bucket, H class)
 __global__ void bin_count_kernel(BinArgs a) {
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < a.num_reads;
@@ -125,9 +138,13 @@ __global__ void bin_count_kernel(BinArgs a) {
         const int g = a.read_record[i];
         const int nh = a.rec_haps[g];
         const int64_t hb = a.rec_hap_base[g];
-        for (int h = 0; h < nh; ++h) atomicAdd(&a.hist[bin_of(a, L, a.hap_lengths[hb + h])], 1u);
+        for (int h = 0; h < nh; ++h) {
+            const int bin = bin_of(a, L, a.hap_lengths[hb + h]);
+            aggregated_add(&a.hist[bin], (unsigned)bin);
+        }
     }
 }
+
 
 // thread per read: scatter items into their sorted slots
 __global__ void bin_scatter_kernel(BinArgs a) {
@@ -140,7 +157,7 @@ __global__ void bin_scatter_kernel(BinArgs a) {
         const int64_t ob = a.rec_pair_base[g] + (int64_t)a.read_local[i] * nh;
         for (int h = 0; h < nh; ++h) {
             const int bin = bin_of(a, L, a.hap_lengths[hb + h]);
-            const unsigned long long pos = atomicAdd(&a.cursor[bin], 1ull);
+            const unsigned long long pos = aggregated_add(&a.cursor[bin], (unsigned)bin);
             a.items[pos] = Task{(int32_t)i, (int32_t)(hb + h), ob + h};
         }
     }

@@ -206,7 +206,8 @@ struct Fp32Wavefront {
                             const float Dold = D[r];
                             N[r] = ls[u] * (Ndiag + Xdiag);
                             D[r] = fmaf(sig[r], Nold, kEps * Dold);
-                            const float In = fmaf(dlt[r], Ndiag, eps[r] * Idiag);
+                            // eps*I carries the serial chain: one FFMA per position
+                            const float In = fmaf(eps[r], Idiag, dlt[r] * Ndiag);
                             Ndiag = Nold;
                             Idiag = In;
                             Xdiag = In + Dold;
@@ -235,7 +236,9 @@ struct Fp32Wavefront {
                         const float bx = __shfl_sync(kFullMask, bcur.x, src, G);
                         const float by = __shfl_sync(kFullMask, bcur.y, src, G);
                         const float bz = __shfl_sync(kFullMask, bcur.z, src, G);
-                        if (t == 0) { Ml = bx; Dl = by; Iul = bz; }
+                        // the border is indexed by row: it feeds the diagonal of the next
+                        // step directly (lanes t > 0 get theirs through the Ml -> Mul rotation)
+                        if (t == 0) { Mul = bx; Dul = by; Iul = bz; }
                         if (src == G - 1) {
                             bcur = bnext;
                             const int64_t idx = (int64_t)k + 1 + G + t;
@@ -261,8 +264,9 @@ struct Fp32Wavefront {
             const float res = log10f(acc) - (log10f(kScale) + log10f(kBeta));
             v.scores[task.out] = res;
             if (degenerate || (v.rescue_enabled && !(acc >= kRescueThreshold && acc <= FLT_MAX))) {
-                const unsigned long long slot = atomicAdd(v.rescue_count, 1ull);
-                v.rescue[slot] = task;
+                const int cls = fp64_class(L);
+                const unsigned long long slot = atomicAdd(v.rescue_count + cls, 1ull);
+                v.rescue[cls][slot] = task;
             }
         }
     }

@@ -1,21 +1,27 @@
-// FP64 rescue pass: the same wavefront in double precision for the pairs
-// whose FP32 result fell below the underflow threshold.
+// FP64 pass: the same wavefront in double precision for the pairs the FP32
+// pass flagged (scaled FP32 sum below the underflow threshold, or an alpha
+// too close to zero for the FP32 kernel's division).
 //
-// Range: along the read the forward values of an unrelated pair fall by about
-// 10^-3.4 per position (10^-850 over 250 bp), beyond even a pre-scaled double.
-// Every lane therefore stores its values as  true * 2^e  with its own integer
-// exponent e.  Every 8 steps a lane renormalises its registers by an exact
+// Range: an unrelated 250 bp read against a 600 bp haplotype lies ~244
+// decades below 1 and long reads reach thousands of decades, beyond a
+// pre-scaled double.  Every lane therefore stores its values as
+// true * 2^e  with its own integer exponent e.  A lane centres its exponent
+// on the first non-zero values it receives (its neighbour may not have
+// renormalised yet), every 8 steps it renormalises its registers by an exact
 // power of two, and every value handed to the next lane travels with the
 // sender's exponent; the receiver multiplies it by 2^(e_recv - e_send).  The
 // result lane keeps its accumulator in its own scale and renormalises it with
-// its registers, so the result is  log10(acc) - e*log10(2) - log10(beta*FLT_MAX/16).
+// its registers, so the result is
+//     log10(acc) - e*log10(2) - log10(beta*FLT_MAX/16).
 // Values more than 2^1022 below the largest value of their lane are dropped;
 // their contribution to the result is below that factor too.
 //
-// One warp (G = 32 lanes, R doubles per lane, T = 32*R positions per tile) per
-// pair.  Reads longer than T run tile after tile; the last lane's
-// (M, Dt, It, exponents) per haplotype row go through a global border buffer,
-// staged through a 32-entry shared ring for lane 0 of the next tile.
+// The recurrence is the plain one (alpha kept, not divided out), so pairs
+// with alpha ~ 0 are exact here.  Work split as in the FP32 kernel: groups of
+// G lanes, R doubles per lane, T = G*R read positions per tile; reads longer
+// than T (MT, G = 32 only) run tile after tile with the last lane's
+// (M, Dt, It, exponents) per haplotype row going through a global border
+// buffer, staged through a 32-entry shared ring for lane 0 of the next tile.
 #pragma once
 
 #include "device_common.cuh"
@@ -35,32 +41,40 @@ __device__ __forceinline__ double pow2i(int k) {
     return __longlong_as_double((long long)(k + 1023) << 52);
 }
 
-template <int R>
+template <int G, int R, bool MT>
 struct Fp64Wavefront {
     static_assert(R % 2 == 0, "R must be even");
-    static constexpr int G = 32;
+    static_assert(!MT || G == 32, "multi-tile FP64 runs one pair per warp");
+    static constexpr int NG = 32 / G;
     static constexpr int T = G * R;
-    static constexpr int Q = R / 2;                 // double2 per thread per table row
+    static constexpr int Q = R / 2;                   // double2 per thread per table row
     static constexpr int kTableDouble2 = 5 * Q * 32;  // per warp
     static constexpr int kRing = 32;
 
-    // One pair per warp.  wtab: this warp's lambda table; ring: kRing entries
-    // of shared memory; scratch: this warp's 2 x rows Border64 in global memory.
-    __device__ static void run(const DevView& v, const Task& task, const float* ph, double2* wtab,
+    // tasks: the warp's ntask (<= NG) items.  wtab: this warp's lambda table;
+    // ring: kRing shared entries (MT); scratch: this warp's 2 x rows Border64.
+    __device__ static void run(const DevView& v, const Task* tasks, int ntask, const float* ph, double2* wtab,
                                Border64* ring, Border64* scratch, int64_t rows) {
-        const int t = threadIdx.x & 31;
+        const int lane = threadIdx.x & 31;
+        const int grp = lane / G;
+        const int t = lane - grp * G;
+        const bool active = grp < ntask;
+        const Task task = tasks[active ? grp : 0];
         const int L = v.read_len[task.read];
         const int H = v.hap_len[task.hap];
-        if (L < 1 || H < 1) return;  // warp-uniform
-        const int ntiles = (L + T - 1) / T;
+        const bool valid = active && L >= 1 && H >= 1;
+        const int Lc = L >= 1 ? L : 1;
+        const int Hc = H >= 1 ? H : 1;
+        const int ntiles = MT ? (Lc + T - 1) / T : 1;  // MT: one group, warp-uniform
         const uint32_t* rpack = v.read_pack + v.read_start[task.read];
         const uint32_t* hw = reinterpret_cast<const uint32_t*>(v.hap_code + v.hap_start[task.hap]);
         const double beta = (double)kBeta;
         const double epsd = (double)kEps;
-        const double Dbound = beta * (double)(kScale / (float)H);
+        const double Dbound = beta * (double)(kScale / (float)Hc);
 
         double acc = 0.0;
         int e = 0;
+        int rlane = -1;
 
         for (int tile = 0; tile < ntiles; ++tile) {
             const bool last = tile == ntiles - 1;
@@ -92,36 +106,40 @@ struct Fp64Wavefront {
                     D[r] = 0.0;
                 }
 #pragma unroll
-                for (int h = 0; h < 5; ++h) wtab[(h * Q + q) * 32 + t] = make_double2(lam[h][0], lam[h][1]);
+                for (int h = 0; h < 5; ++h) wtab[(h * Q + q) * 32 + lane] = make_double2(lam[h][0], lam[h][1]);
             }
             e = 0;
             int t_res = 0, r_res = 0;
             if (last) {
-                const int rel = L - 1 - tile * T;
+                const int rel = Lc - 1 - tile * T;
                 t_res = rel / R;
                 r_res = rel - t_res * R;
             }
-            const int kg = last ? H + t_res : H + G - 1;
-            const bool res_lane = last && t == t_res;
+            const int kg = last ? Hc + t_res : Hc + G - 1;
+            const bool res_lane = valid && last && t == t_res;
             const bool addM = r_res == R - 1;
-            const int K = (kg + 1 + 3) & ~3;
+            if (res_lane) rlane = t;
+            const int kmax = (int)__reduce_max_sync(kFullMask, (unsigned)(valid ? kg : 0));
+            const int K = (kmax + 1 + 3) & ~3;
 
             double Ml = 0.0, Dl = 0.0, Mul = 0.0, Dul = 0.0, Iul = 0.0;
             int eMl = 0, eMul = 0, eIul = 0;
             if (t == 0 && tile == 0) { Dl = Dbound; Dul = Dbound; }
+            bool empty = !(t == 0 && tile == 0);
             const Border64* ein = scratch + ((tile - 1) & 1) * rows;
             Border64* eout = scratch + (tile & 1) * rows;
-            const bool writer = !last && t == G - 1;
+            const bool writer = MT && valid && !last && t == G - 1;
             Border64 nb{0.0, 0.0, 0.0, 0, 0};
-            if (tile > 0 && t < rows) nb = ein[t];
+            if (MT && tile > 0 && t < rows) nb = ein[t];
             int h = 4;
 
-            const int wlast = ((H + 15) & ~15) / 4 - 1;
+            // code words of this group's haplotype, clamped to its own extent
+            const int wlast = ((Hc + 15) & ~15) / 4 - 1;
             uint32_t wcur = __ldg(hw);
             uint32_t wnext = __ldg(hw + 1);
             for (int k0 = 0; k0 < K; k0 += 4) {
                 const uint32_t wpref = __ldg(hw + min_i((k0 >> 2) + 2, wlast));
-                if (tile > 0 && (k0 & (kRing - 1)) == 0) {
+                if (MT && tile > 0 && (k0 & (kRing - 1)) == 0) {
                     __syncwarp();
                     ring[t] = nb;
                     __syncwarp();
@@ -131,10 +149,16 @@ struct Fp64Wavefront {
 #pragma unroll
                 for (int s = 0; s < 4; ++s) {
                     const int k = k0 + s;
-                    int hn = __shfl_up_sync(kFullMask, h, 1);
+                    int hn = __shfl_up_sync(kFullMask, h, 1, G);
                     if (t == 0) hn = (int)((wcur >> (8 * s)) & 0xffu);
                     h = hn;
-                    const double2* trow = wtab + h * (Q * 32) + t;
+                    if (empty && (Mul != 0.0 || Dul != 0.0 || Iul != 0.0)) {
+                        // centre this lane's scale on the first values it receives
+                        const double md = fmax(fabs(Mul), fabs(Dul));
+                        e = md != 0.0 ? eMul - ilogb(md) : eIul - ilogb(fabs(Iul));
+                        empty = false;
+                    }
+                    const double2* trow = wtab + h * (Q * 32) + lane;
                     const double fM = pow2i(e - eMul);
                     const double fI = pow2i(e - eIul);
                     double Mdiag = Mul * fM;
@@ -151,7 +175,7 @@ struct Fp64Wavefront {
                             const double Dold = D[r];
                             M[r] = ls[u] * fma(alpha[r], Mdiag, Xdiag);
                             D[r] = fma(sig[r], Mold, epsd * Dold);
-                            const double In = fma(dlt[r], Mdiag, eps[r] * Idiag);
+                            const double In = fma(eps[r], Idiag, dlt[r] * Mdiag);
                             Mdiag = Mold;
                             Idiag = In;
                             Xdiag = In + Dold;
@@ -163,24 +187,25 @@ struct Fp64Wavefront {
                     }
                     if (writer) {
                         const int j = k - (G - 1);
-                        if (j >= 0 && j < H) { eout[j].m = M[R - 1]; eout[j].d = D[R - 1]; eout[j].e = e; }
-                        if (j >= 1 && j - 1 < H) { eout[j - 1].i = Idiag; eout[j - 1].ei = e; }
+                        if (j >= 0 && j < Hc) { eout[j].m = M[R - 1]; eout[j].d = D[R - 1]; eout[j].e = e; }
+                        if (j >= 1 && j - 1 < Hc) { eout[j - 1].i = Idiag; eout[j - 1].ei = e; }
                     }
                     // hand-off: values travel with the sender's exponent
                     Mul = Ml; Dul = Dl; eMul = eMl;
-                    Ml = __shfl_up_sync(kFullMask, M[R - 1], 1);
-                    Dl = __shfl_up_sync(kFullMask, D[R - 1], 1);
-                    Iul = __shfl_up_sync(kFullMask, Idiag, 1);
-                    const int es = __shfl_up_sync(kFullMask, e, 1);
+                    Ml = __shfl_up_sync(kFullMask, M[R - 1], 1, G);
+                    Dl = __shfl_up_sync(kFullMask, D[R - 1], 1, G);
+                    Iul = __shfl_up_sync(kFullMask, Idiag, 1, G);
+                    const int es = __shfl_up_sync(kFullMask, e, 1, G);
                     eMl = es;
                     eIul = es;
                     if (t == 0) {
-                        if (tile > 0) {
-                            if (k < H) {
+                        if (MT && tile > 0) {
+                            // the border is indexed by row: it feeds the next step's diagonal
+                            if (k < Hc) {
                                 const Border64 b = ring[k & (kRing - 1)];
-                                Ml = b.m; Dl = b.d; eMl = b.e; Iul = b.i; eIul = b.ei;
+                                Mul = b.m; Dul = b.d; eMul = b.e; Iul = b.i; eIul = b.ei;
                             } else {
-                                Ml = 0.0; Dl = 0.0; Iul = 0.0; eMl = 0; eIul = 0;
+                                Mul = 0.0; Dul = 0.0; Iul = 0.0; eMul = 0; eIul = 0;
                             }
                         } else {
                             Ml = 0.0; Dl = Dbound; Iul = 0.0; eMl = 0; eIul = 0;
@@ -209,8 +234,7 @@ struct Fp64Wavefront {
             }
             __syncwarp();
         }
-        const int rel = L - 1 - (ntiles - 1) * T;
-        if (t == rel / R) {
+        if (valid && t == rlane) {
             double res = -INFINITY;
             if (acc > 0.0)
                 res = log10(acc) - (double)e * 0.30102999566398119521 - log10((double)kScale) -

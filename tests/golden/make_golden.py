@@ -77,10 +77,11 @@ def ref_gpu_inputs() -> dict[str, str]:
     return cases
 
 
-def ref_gpu(binary: Path) -> None:
+def ref_gpu(binary: Path, outdir: Path) -> None:
+    outdir.mkdir(parents=True, exist_ok=True)
     for name, text in ref_gpu_inputs().items():
-        inp = HERE / f"ref_gpu_{name}.in"
-        out = HERE / f"ref_gpu_{name}.out"
+        inp = outdir / f"ref_gpu_{name}.in"
+        out = outdir / f"ref_gpu_{name}.out"
         inp.write_text(text)
         subprocess.run([str(binary), "--inputfile", str(inp), "--outputfile", str(out)], check=True,
                        stdout=subprocess.DEVNULL)
@@ -92,11 +93,12 @@ def main() -> None:
     ap.add_argument("--reference-dir", default="/root/reference")
     ap.add_argument("--ref-gpu", action="store_true", help="run the reference GPU binary (needs a GPU)")
     ap.add_argument("--binary", default=str(ROOT / "oracle" / "_ref" / "gpuPairHMM"))
+    ap.add_argument("--outdir", default=str(HERE))
     a = ap.parse_args()
     if Path(a.reference_dir).is_dir():
         readme_example(Path(a.reference_dir))
     if a.ref_gpu:
-        ref_gpu(Path(a.binary))
+        ref_gpu(Path(a.binary), Path(a.outdir))
 
 
 if __name__ == "__main__":

@@ -68,7 +68,9 @@ def test_length_sweep_across_tile_boundaries(engine, plain_engine):
     b = _soa(recs)
     want = oracle.batch_log10(b)
     assert_log10_close(engine.compute(b), want, what="sweep engine")
-    assert_log10_close(plain_engine.compute(b), want, what="sweep plain")
+    # the plain form is FP32 only, like the reference: compare it in FP32 range
+    ok = want > -60.0
+    assert_log10_close(plain_engine.compute(b)[ok], want[ok], what="sweep plain")
 
 
 def test_haplotype_length_sweep(engine):
@@ -138,6 +140,18 @@ def test_very_long_read_many_tiles(engine):
     recs = [_record(rng, 4500, 5200, n_reads=2, n_haps=1), _record(rng, 2049, 300, n_reads=1, n_haps=2)]
     b = _soa(recs)
     assert_log10_close(engine.compute(b), oracle.batch_log10(b), what="long read")
+
+
+def test_fp64_long_reads_short_haplotypes(engine):
+    """Insertion-dominated pairs: every read position costs about a factor 10,
+    so the FP64 pass carries values across hundreds of decades per tile."""
+    rng = np.random.default_rng(21)
+    recs = [_record(rng, L, H, n_reads=2, n_haps=2, related=False)
+            for L, H in [(257, 1), (300, 2), (383, 3), (500, 4), (641, 5), (900, 1), (1300, 3), (2100, 7)]]
+    b = _soa(recs)
+    want = oracle.batch_log10(b)
+    assert want.min() < -600
+    assert_log10_close(engine.compute(b), want, what="long reads, short haplotypes")
 
 
 def test_empty_and_ragged_records(engine):
