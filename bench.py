@@ -51,7 +51,9 @@ def parse_args():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--impl", choices=["ours", "reference", "reference-gpu", "cli"], default="ours",
+                    help="reference-gpu / cli: the reference's gpuPairHMM binary (oracle/_ref, built from its "
+                         "sources) or our CLI on the same record file, GCUPS as the binary prints it")
     ap.add_argument("--mode", choices=["engine", "plain"], default="engine")
     ap.add_argument("--regions", type=int, default=20000)
     ap.add_argument("--seed", type=int, default=1)
@@ -200,6 +202,41 @@ def run_reference(args, cfg):
     print(json.dumps(line), flush=True)
 
 
+def run_binary(args, cfg):
+    """A gpuPairHMM-style binary on a record file of the workload (file parse,
+    upload, compute, download; output to /dev/null as the reference skips
+    formatting for it).  GCUPS as printed by the binary."""
+    import re
+    from gpupairhmm_b200 import synth, CLI_PATH
+    binary = ROOT / "oracle" / "_ref" / "gpuPairHMM" if args.impl == "reference-gpu" else CLI_PATH
+    if not binary.exists():
+        print(json.dumps({"impl": args.impl, "unavailable": f"{binary} not built"}))
+        return
+    batch = synth.config1(seed=args.seed, regions=args.regions)
+    fd, path = tempfile.mkstemp(prefix="records_", suffix=".txt")
+    os.close(fd)
+    try:
+        Path(path).write_text(synth.to_text(batch))
+        vals = []
+        for i in range(args.warmup + args.steps):
+            out = subprocess.run([str(binary), "--inputfile", path, "--outputfile", "/dev/null",
+                                  "--fileBatchsize", "0", "--transferBatchsize", "0"],
+                                 capture_output=True, text=True, check=True).stdout
+            m = re.search(r"Batch processing time: ([0-9.e+-]+)s \(([0-9.e+-]+) GCUPS\)", out)
+            if i >= args.warmup:
+                vals.append((float(m.group(1)), float(m.group(2))))
+    finally:
+        os.unlink(path)
+    secs = sum(v[0] for v in vals)
+    value = batch.cells() * len(vals) / secs / 1e9
+    print(json.dumps({"impl": args.impl, "metric": METRIC, "value": round(value, 3), "unit": "GCUPS",
+                      "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+                      "ms_per_step": round(secs / len(vals) * 1e3, 3), "higher_is_better": True,
+                      "data": "synthetic", "config": dict(cfg, pairs=batch.num_pairs, cells=batch.cells()),
+                      "timing": "the binary's own batch wall clock (upload, kernels, download; file "
+                                "parsing excluded), whole batch at once"}), flush=True)
+
+
 def run_ours(args, cfg, rank, world, local_rank):
     import torch
     import gpupairhmm_b200 as g
@@ -312,6 +349,10 @@ def main():
         if rank != 0:
             return
         run_reference(args, cfg)
+        return
+    if args.impl in ("reference-gpu", "cli"):
+        if rank == 0:
+            run_binary(args, cfg)
         return
     run_ours(args, cfg, rank, world, local_rank)
 

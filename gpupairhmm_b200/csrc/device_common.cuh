@@ -23,9 +23,15 @@ constexpr float kBeta = 0.9f;
 constexpr float kEps = 0.1f;
 constexpr float kScale = FLT_MAX / 16.0f;
 
-// Scaled FP32 sums below this are treated as underflowed and recomputed in
-// FP64: every cell value whose rounding could matter is then a normal float.
-constexpr float kRescueThreshold = 0x1p-100f;
+// FP64 recompute threshold.  Each path reaches the last read row at most
+// once and transitions never exceed 1, so a value's share of the result is at
+// most the value itself; cells that round in the denormal range (absolute
+// error <= 2^-150 each, 3 states per cell) therefore move the scaled sum S by
+// at most 3*L*H*2^-150.  S >= 3*L*H*2^-127 keeps that below 2^-23 relative;
+// smaller sums go to the FP64 pass.
+__host__ __device__ __forceinline__ float rescue_threshold(int L, int H) {
+    return 3.0f * (float)L * (float)H * 0x1p-127f;
+}
 
 // The FP32 kernel divides by alpha = 1 - (delta + sigma); pairs with a smaller
 // |alpha| anywhere go to the FP64 pass instead.
@@ -50,8 +56,8 @@ struct DevView {
     const int64_t* hap_start;  // in bytes, multiple of 16
     const int32_t* hap_len;
     float* scores;
-    Task* rescue[3];            // flagged pairs by read-length class (fp64_class)
-    unsigned long long* rescue_count;  // [3]
+    Task* rescue[5];            // flagged pairs by read-length class (fp64_class)
+    unsigned long long* rescue_count;  // [kFp64Classes]
     int rescue_enabled;
     const float* ph2pr;         // 128 floats in global memory
 };
@@ -63,12 +69,12 @@ __device__ __forceinline__ uint32_t code_of(uint8_t c) {
 
 __device__ __forceinline__ int min_i(int a, int b) { return a < b ? a : b; }
 
-// FP64 pass classes: reads up to 64 and 128 positions run 4 and 2 pairs per
-// warp (single tile); longer reads one pair per warp, multi-tile.
-constexpr int kFp64ClassMax0 = 64;
-constexpr int kFp64ClassMax1 = 128;
+// FP64 pass length classes (tile = G x R): 64 = 8x8, 96 = 16x6, 128 = 16x8,
+// 192 = 32x6, then 32x8 multi-tile for longer reads.
+constexpr int kFp64Classes = 5;
+constexpr int kFp64ClassMax[kFp64Classes - 1] = {64, 96, 128, 192};
 __host__ __device__ __forceinline__ int fp64_class(int L) {
-    return L <= kFp64ClassMax0 ? 0 : (L <= kFp64ClassMax1 ? 1 : 2);
+    return L <= 64 ? 0 : L <= 96 ? 1 : L <= 128 ? 2 : L <= 192 ? 3 : 4;
 }
 
 }  // namespace phmm

@@ -25,15 +25,11 @@ namespace {
 constexpr int64_t kScratchBudget = int64_t(4) << 30;  // border scratch cap per batch
 
 std::vector<TileRule> engine_default_rules() {
-    // Tile per read-length bucket for the persistent engine.  Replaced at
-    // start-up by the tuned table when one is provided.
+    // Tile per read-length bucket for the persistent engine, measured on a B200
+    // by gpupairhmm_b200/autotune.py (every compiled configuration timed on each
+    // 16-position length class; adjacent classes with one winner merged).
     return {
-        {32, 4, 8, false},     {48, 4, 12, false},    {64, 4, 16, false},    {80, 4, 20, false},
-        {96, 4, 24, false},    {112, 4, 28, false},   {128, 4, 32, false},   {160, 8, 20, false},
-        {192, 8, 24, false},   {224, 8, 28, false},   {256, 8, 32, false},   {320, 16, 20, false},
-        {384, 16, 24, false},  {448, 16, 28, false},  {512, 16, 32, false},  {640, 32, 20, false},
-        {768, 32, 24, false},  {896, 32, 28, false},  {1024, 32, 32, false}, {1280, 32, 20, true},
-        {1536, 32, 24, true},  {1792, 32, 28, true},  {2048, 32, 32, true},  {1 << 30, 32, 32, true},
+#include "tuned_table.inc"
     };
 }
 
@@ -138,7 +134,7 @@ pairhmm_status_t Engine::init() {
     // dynamic shared memory opt-in for every kernel on this device
     for (const ConfigInfo& c : fp32_configs())
         PHMM_CUDA(cudaFuncSetAttribute(c.kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c.smem_bytes));
-    for (int c = 0; c < 3; ++c)
+    for (int c = 0; c < kFp64Classes; ++c)
         PHMM_CUDA(cudaFuncSetAttribute(fp64_kernel(c), cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)fp64_smem_bytes(c)));
 
@@ -147,7 +143,7 @@ pairhmm_status_t Engine::init() {
     for (int i = 0; i < 128; ++i) table[i] = (float)std::pow(10.0, (-i) / 10.0);
     PHMM_CUDA(ph2pr_.ensure(sizeof(table)));
     PHMM_CUDA(cudaMemcpy(ph2pr_.ptr, table, sizeof(table), cudaMemcpyHostToDevice));
-    PHMM_CUDA(counters_.ensure(sizeof(unsigned long long) * (kMaxBuckets + 8)));
+    PHMM_CUDA(counters_.ensure(sizeof(unsigned long long) * (kMaxBuckets + 2 * kFp64Classes)));
     PHMM_CUDA(sched_.ensure(sizeof(Schedule)));
     ready_ = true;
     return upload_rules();
@@ -415,7 +411,7 @@ pairhmm_status_t Engine::enqueue_pipeline(const pairhmm_batch_t& in, const Batch
     if (stage == 0) {
     PHMM_CUDA(launch_binning(ba, prep_grid, s, per_task_.as<int>(), config_.as<int>(), sched_.as<Schedule>(), nb));
     launches_ += 4;
-    PHMM_CUDA(cudaMemsetAsync(counters_.ptr, 0, sizeof(unsigned long long) * (kMaxBuckets + 8), s));
+    PHMM_CUDA(cudaMemsetAsync(counters_.ptr, 0, sizeof(unsigned long long) * (kMaxBuckets + 2 * kFp64Classes), s));
     return PAIRHMM_OK;
     }
 
@@ -430,7 +426,7 @@ pairhmm_status_t Engine::enqueue_pipeline(const pairhmm_batch_t& in, const Batch
     v.scores = d_scores;
     {
         int64_t off = 0;
-        for (int c = 0; c < 3; ++c) {
+        for (int c = 0; c < kFp64Classes; ++c) {
             v.rescue[c] = rescue_.as<Task>() + off;
             off += x.class_pairs[c];
         }
@@ -461,14 +457,14 @@ pairhmm_status_t Engine::enqueue_pipeline(const pairhmm_batch_t& in, const Batch
     return PAIRHMM_OK;
     }
     // stage 2: FP64 pass over flagged pairs (FP32 underflow, or degenerate alpha)
-    for (int c = 0; c < 3; ++c) {
+    for (int c = 0; c < kFp64Classes; ++c) {
         if (x.class_pairs[c] == 0) continue;
         Fp64LaunchArgs fa{};
         fa.view = v;
         fa.cls = c;
         fa.items = v.rescue[c];
         fa.count = counters + kMaxBuckets + c;
-        fa.counter = counters + kMaxBuckets + 3 + c;
+        fa.counter = counters + kMaxBuckets + kFp64Classes + c;
         fa.scratch = scratch_.ptr;
         fa.rows = plan.rows;
         fa.grid = plan.fp64_grid[c];
@@ -504,7 +500,7 @@ Engine::Plan Engine::make_plan(const BatchIndex& x) const {
         // the plain form runs one task per warp; a grid capped by scratch loops on the counter
         p.persistent[b] = (!plain || grid < need_blocks) ? 1 : 0;
     }
-    for (int c = 0; c < 3; ++c) {
+    for (int c = 0; c < kFp64Classes; ++c) {
         int64_t grid = persistent_grid(fp64_kernel(c), fp64_smem_bytes(c));
         const int64_t per_warp = (int64_t)fp64_scratch_bytes_per_row(c) * p.rows;
         if (per_warp > 0) {
@@ -619,9 +615,9 @@ pairhmm_status_t Engine::compute_host(const pairhmm_batch_t& b, float* scores) {
     PHMM_CUDA(cudaEventRecord(ev0_, s));
     if ((st = run_pipeline(dev, x, scores_.as<float>(), s)) != PAIRHMM_OK) return st;
     PHMM_CUDA(cudaMemcpyAsync(scores, scores_.ptr, 4 * x.num_pairs, cudaMemcpyDeviceToHost, s));
-    unsigned long long rescued3[3] = {0, 0, 0};
-    PHMM_CUDA(cudaMemcpyAsync(rescued3, counters_.as<unsigned long long>() + kMaxBuckets, sizeof(rescued3),
-                              cudaMemcpyDeviceToHost, s));
+    unsigned long long rescued_by_class[kFp64Classes] = {};
+    PHMM_CUDA(cudaMemcpyAsync(rescued_by_class, counters_.as<unsigned long long>() + kMaxBuckets,
+                              sizeof(rescued_by_class), cudaMemcpyDeviceToHost, s));
     PHMM_CUDA(cudaStreamSynchronize(s));
     float ms = 0.f, a = 0.f, b2 = 0.f, c = 0.f;
     PHMM_CUDA(cudaEventElapsedTime(&ms, ev0_, ev1_));
@@ -634,8 +630,9 @@ pairhmm_status_t Engine::compute_host(const pairhmm_batch_t& b, float* scores) {
     stats_.fp64_ms = c;
     stats_.launches = launches_;
     stats_.h2d_bytes = 4 * rn + hn + 12 * x.num_reads + 12 * x.num_haps + index_bytes(x);
-    stats_.d2h_bytes = 4 * x.num_pairs + (int64_t)sizeof(rescued3);
-    stats_.rescued = (int64_t)(rescued3[0] + rescued3[1] + rescued3[2]);
+    stats_.d2h_bytes = 4 * x.num_pairs + (int64_t)sizeof(rescued_by_class);
+    stats_.rescued = 0;
+    for (unsigned long long r : rescued_by_class) stats_.rescued += (int64_t)r;
     stats_.total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     return PAIRHMM_OK;
 }

@@ -31,7 +31,7 @@ struct BatchIndex {
     std::vector<int32_t> read_record, read_local, rec_haps;
     std::vector<int64_t> rec_hap_base, rec_pair_base, read_start, hap_start;
     std::vector<int64_t> bucket_pairs;              // by bucket index
-    int64_t class_pairs[3] = {0, 0, 0};             // by FP64 length class (fp64_class)
+    int64_t class_pairs[kFp64Classes] = {};         // by FP64 length class (fp64_class)
     int64_t multi_tile_pairs = 0;
 };
 
@@ -78,7 +78,7 @@ private:
         int64_t rows = 0;                 // border rows per buffer
         std::vector<int> grid;            // by bucket
         std::vector<int> persistent;      // by bucket
-        int fp64_grid[3] = {0, 0, 0};   // by FP64 length class
+        int fp64_grid[kFp64Classes] = {};   // by FP64 length class
         size_t scratch_bytes = 0;
     };
     Plan make_plan(const BatchIndex& idx) const;

@@ -35,9 +35,13 @@ const ConfigInfo* find_fp32_config(int G, int R, bool multi_tile) {
 
 // ---------------------------------------------------------------- FP64 pass
 using W64c0 = Fp64Wavefront<8, 8, false>;
-using W64c1 = Fp64Wavefront<16, 8, false>;
-using W64c2 = Fp64Wavefront<32, 8, true>;
-static_assert(W64c0::T == kFp64ClassMax0 && W64c1::T == kFp64ClassMax1, "class bounds follow the tiles");
+using W64c1 = Fp64Wavefront<16, 6, false>;
+using W64c2 = Fp64Wavefront<16, 8, false>;
+using W64c3 = Fp64Wavefront<32, 6, false>;
+using W64c4 = Fp64Wavefront<32, 8, true>;
+static_assert(W64c0::T == kFp64ClassMax[0] && W64c1::T == kFp64ClassMax[1] && W64c2::T == kFp64ClassMax[2] &&
+                  W64c3::T == kFp64ClassMax[3],
+              "class bounds follow the tiles");
 
 template <class W>
 __global__ void __launch_bounds__(kBlockThreads)
@@ -73,29 +77,27 @@ size_t fp64_smem_for() {
            (size_t)kWarpsPerBlock * W::kRing * sizeof(Border64);
 }
 
-size_t fp64_smem_bytes(int cls) {
-    return cls == 0 ? fp64_smem_for<W64c0>() : cls == 1 ? fp64_smem_for<W64c1>() : fp64_smem_for<W64c2>();
-}
-size_t fp64_scratch_bytes_per_row(int cls) { return cls == 2 ? 2 * sizeof(Border64) : 0; }
+#define PHMM_FP64_DISPATCH(cls, EXPR)      \
+    switch (cls) {                          \
+        case 0: { using W = W64c0; EXPR; }  \
+        case 1: { using W = W64c1; EXPR; }  \
+        case 2: { using W = W64c2; EXPR; }  \
+        case 3: { using W = W64c3; EXPR; }  \
+        default: { using W = W64c4; EXPR; } \
+    }
+
+size_t fp64_smem_bytes(int cls) { PHMM_FP64_DISPATCH(cls, return fp64_smem_for<W>()); }
+size_t fp64_scratch_bytes_per_row(int cls) { return cls == kFp64Classes - 1 ? 2 * sizeof(Border64) : 0; }
 const void* fp64_kernel(int cls) {
-    return cls == 0 ? reinterpret_cast<const void*>(&fp64_rescue_kernel<W64c0>)
-         : cls == 1 ? reinterpret_cast<const void*>(&fp64_rescue_kernel<W64c1>)
-                    : reinterpret_cast<const void*>(&fp64_rescue_kernel<W64c2>);
+    PHMM_FP64_DISPATCH(cls, return reinterpret_cast<const void*>(&fp64_rescue_kernel<W>));
 }
-int fp64_per_warp(int cls) { return cls == 0 ? W64c0::NG : cls == 1 ? W64c1::NG : W64c2::NG; }
+int fp64_per_warp(int cls) { PHMM_FP64_DISPATCH(cls, return W::NG); }
 
 cudaError_t launch_fp64_rescue(const Fp64LaunchArgs& a) {
-    Border64* scr = static_cast<Border64*>(a.scratch);
-    if (a.cls == 0)
-        fp64_rescue_kernel<W64c0><<<a.grid, kBlockThreads, fp64_smem_bytes(0), a.stream>>>(
-            a.view, a.items, a.count, a.counter, nullptr, a.rows);
-    else if (a.cls == 1)
-        fp64_rescue_kernel<W64c1><<<a.grid, kBlockThreads, fp64_smem_bytes(1), a.stream>>>(
-            a.view, a.items, a.count, a.counter, nullptr, a.rows);
-    else
-        fp64_rescue_kernel<W64c2><<<a.grid, kBlockThreads, fp64_smem_bytes(2), a.stream>>>(
-            a.view, a.items, a.count, a.counter, scr, a.rows);
-    return cudaGetLastError();
+    Border64* scr = a.cls == kFp64Classes - 1 ? static_cast<Border64*>(a.scratch) : nullptr;
+    PHMM_FP64_DISPATCH(a.cls, (fp64_rescue_kernel<W><<<a.grid, kBlockThreads, fp64_smem_bytes(a.cls), a.stream>>>(
+                                   a.view, a.items, a.count, a.counter, scr, a.rows));
+                       return cudaGetLastError());
 }
 
 // ---------------------------------------------------------------- preparation

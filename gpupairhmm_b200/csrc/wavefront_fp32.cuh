@@ -263,7 +263,7 @@ struct Fp32Wavefront {
         if (valid && t == rlane) {
             const float res = log10f(acc) - (log10f(kScale) + log10f(kBeta));
             v.scores[task.out] = res;
-            if (degenerate || (v.rescue_enabled && !(acc >= kRescueThreshold && acc <= FLT_MAX))) {
+            if (degenerate || (v.rescue_enabled && !(acc >= rescue_threshold(L, H) && acc <= FLT_MAX))) {
                 const int cls = fp64_class(L);
                 const unsigned long long slot = atomicAdd(v.rescue_count + cls, 1ull);
                 v.rescue[cls][slot] = task;

@@ -7,7 +7,7 @@
 // pre-scaled double.  Every lane therefore stores its values as
 // true * 2^e  with its own integer exponent e.  A lane centres its exponent
 // on the first non-zero values it receives (its neighbour may not have
-// renormalised yet), every 8 steps it renormalises its registers by an exact
+// renormalised yet), every 16 steps it renormalises its registers by an exact
 // power of two, and every value handed to the next lane travels with the
 // sender's exponent; the receiver multiplies it by 2^(e_recv - e_send).  The
 // result lane keeps its accumulator in its own scale and renormalises it with
@@ -152,7 +152,8 @@ struct Fp64Wavefront {
                     int hn = __shfl_up_sync(kFullMask, h, 1, G);
                     if (t == 0) hn = (int)((wcur >> (8 * s)) & 0xffu);
                     h = hn;
-                    if (empty && (Mul != 0.0 || Dul != 0.0 || Iul != 0.0)) {
+                    // lanes fill during the first pass of the wavefront (k < G + 8)
+                    if (k0 < G + 8 && empty && (Mul != 0.0 || Dul != 0.0 || Iul != 0.0)) {
                         // centre this lane's scale on the first values it receives
                         const double md = fmax(fabs(Mul), fabs(Dul));
                         e = md != 0.0 ? eMul - ilogb(md) : eIul - ilogb(fabs(Iul));
@@ -211,8 +212,9 @@ struct Fp64Wavefront {
                             Ml = 0.0; Dl = Dbound; Iul = 0.0; eMl = 0; eIul = 0;
                         }
                     }
-                    // renormalise this lane every 8 steps (exact powers of two)
-                    if ((k & 7) == 7) {
+                    // renormalise every 16 steps (exact powers of two); a value moves by at
+                    // most 2^13 per row, so lanes stay within 2^300 of their scale meanwhile
+                    if ((k & 15) == 15) {
                         double mx = res_lane ? fabs(acc) : 0.0;
 #pragma unroll
                         for (int r = 0; r < R; ++r) mx = fmax(mx, fmax(fabs(M[r]), fabs(D[r])));
