@@ -330,15 +330,17 @@ class Engine:
         return out[:num_scores]
 
     # ------------------------------------------------------------ tuning
-    def tile_table(self) -> list[tuple[int, int, int, bool]]:
+    def tile_table(self) -> list[tuple[int, int, int, int]]:
+        """(max read length, G, R, kind) with kind 0 = one tile, 1 = multi-tile,
+        2 = one tile, two reads per group in packed FP32."""
         n = ctypes.c_int32()
         _check(lib().pairhmm_get_tile_table(self._h, None, None, None, None, 0, ctypes.byref(n)), self._h)
         arrs = [np.zeros(n.value, dtype=np.int32) for _ in range(4)]
         _check(lib().pairhmm_get_tile_table(self._h, *[_ptr(a) for a in arrs], n.value, ctypes.byref(n)), self._h)
-        return [(int(a), int(b), int(c), bool(d)) for a, b, c, d in zip(*arrs)]
+        return [(int(a), int(b), int(c), int(d)) for a, b, c, d in zip(*arrs)]
 
     def set_tile_table(self, rules) -> None:
-        arrs = [np.array([r[i] for r in rules], dtype=np.int32) for i in range(4)]
+        arrs = [np.array([int(r[i]) for r in rules], dtype=np.int32) for i in range(4)]
         _check(lib().pairhmm_set_tile_table(self._h, *[_ptr(a) for a in arrs], len(rules)), self._h)
 
 

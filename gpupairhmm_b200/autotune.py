@@ -31,6 +31,7 @@ HERE = Path(__file__).resolve().parent
 SINGLE = [(G, R) for G in (4, 8, 16, 32) for R in (4, 8, 12, 16, 20, 24, 28, 32)
           if not (G >= 8 and R == 4)]
 MULTI = [(32, 16), (32, 20), (32, 24), (32, 28), (32, 32), (16, 32)]
+PACKED = [(G, R) for G in (4, 8, 16, 32) for R in (8, 12, 16)]  # two reads per group, packed FP32
 
 
 def classes():
@@ -64,9 +65,10 @@ def class_batch(lo: int, hi: int, pairs: int, seed: int) -> Batch:
     return b.build()
 
 
-def time_config(engine: Engine, batch: Batch, G: int, R: int, mt: bool, repeats: int) -> float:
-    """GCUPS of the FP32 launches for this configuration on this batch."""
-    engine.set_tile_table([(1 << 30, G, R, mt)] if mt else [(G * R, G, R, False), (1 << 30, 32, 32, True)])
+def time_config(engine: Engine, batch: Batch, G: int, R: int, kind: int, repeats: int) -> float:
+    """GCUPS of the FP32 launches for this configuration (kind 0 one tile,
+    1 multi-tile, 2 packed) on this batch."""
+    engine.set_tile_table([(1 << 30, G, R, 1)] if kind == 1 else [(G * R, G, R, kind), (1 << 30, 32, 32, 1)])
     engine.compute(batch)
     best = 0.0
     for _ in range(repeats):
@@ -78,14 +80,16 @@ def time_config(engine: Engine, batch: Batch, G: int, R: int, mt: bool, repeats:
 
 def tune(pairs_per_class: int = 6000, repeats: int = 3, device: int = 0):
     eng = Engine(device=device, fp64_rescue=False)
+    eng.set_tile_table([(1 << 30, 32, 32, 1)])
     results = []
     for ci, (lo, hi) in enumerate(classes()):
         batch = class_batch(lo, hi, pairs_per_class if hi <= 1024 else max(512, pairs_per_class // 8), 1000 + ci)
-        cands = [(G, R, False) for G, R in SINGLE if G * R >= hi] if hi <= 1024 else []
-        cands += [(G, R, True) for G, R in MULTI if hi > 1024 or G * R < hi]
+        cands = [(G, R, 0) for G, R in SINGLE if G * R >= hi] if hi <= 1024 else []
+        cands += [(G, R, 2) for G, R in PACKED if G * R >= hi]
+        cands += [(G, R, 1) for G, R in MULTI if hi > 1024 or G * R < hi]
         timings = {}
-        for G, R, mt in cands:
-            timings[f"{G}x{R}{'mt' if mt else ''}"] = time_config(eng, batch, G, R, mt, repeats)
+        for G, R, kind in cands:
+            timings[f"{G}x{R}{['', 'mt', 'p'][kind]}"] = time_config(eng, batch, G, R, kind, repeats)
         best = max(timings, key=timings.get)
         results.append({"lo": lo, "hi": hi, "best": best, "gcups": timings})
         print(f"[{lo:5d},{hi:5d}] best {best:10s} {timings[best]:8.1f} GCUPS "
@@ -98,28 +102,31 @@ def to_rules(results):
     rules = []
     for r in results:
         key = r["best"]
-        mt = key.endswith("mt")
-        G, R = (int(x) for x in key.replace("mt", "").split("x"))
-        if rules and (rules[-1][1], rules[-1][2], rules[-1][3]) == (G, R, mt):
-            rules[-1] = (r["hi"], G, R, mt)
+        kind = 1 if key.endswith("mt") else (2 if key.endswith("p") else 0)
+        G, R = (int(x) for x in key.replace("mt", "").replace("p", "").split("x"))
+        if rules and (rules[-1][1], rules[-1][2], rules[-1][3]) == (G, R, kind):
+            rules[-1] = (r["hi"], G, R, kind)
         else:
-            rules.append((r["hi"], G, R, mt))
+            rules.append((r["hi"], G, R, kind))
     last = rules[-1]
-    rules[-1] = (1 << 30, last[1], last[2], True) if last[3] else last
-    if not rules[-1][3]:
-        rules.append((1 << 30, 32, 32, True))
+    if last[3] == 1:
+        rules[-1] = (1 << 30, last[1], last[2], 1)
+    else:
+        rules.append((1 << 30, 32, 32, 1))
     return rules
 
 
 def write_outputs(results, rules):
     meta = {"device": "NVIDIA B200", "when": time.strftime("%Y-%m-%dT%H:%M:%SZ", time.gmtime()),
-            "rules": [{"max_len": a, "G": b, "R": c, "multi_tile": d} for a, b, c, d in rules],
+            "rules": [{"max_len": a, "G": b, "R": c, "kind": ["single", "multi_tile", "packed"][d]}
+                      for a, b, c, d in rules],
             "classes": results}
     (HERE / "tuning_sm100a.json").write_text(json.dumps(meta, indent=1))
     lines = ["// Generated by gpupairhmm_b200/autotune.py on a B200; see tuning_sm100a.json.",
-             "// {max read length, G, R, multi-tile}"]
+             "// {max read length, G, R, multi-tile, packed}"]
     for a, b, c, d in rules:
-        lines.append(f"{{{a if a < (1 << 30) else '1 << 30'}, {b}, {c}, {'true' if d else 'false'}}},")
+        lines.append(f"{{{a if a < (1 << 30) else '1 << 30'}, {b}, {c}, {'true' if d == 1 else 'false'}, "
+                     f"{'true' if d == 2 else 'false'}}},")
     (HERE / "csrc" / "tuned_table.inc").write_text("\n".join(lines) + "\n")
 
 

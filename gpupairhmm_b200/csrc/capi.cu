@@ -170,7 +170,7 @@ pairhmm_status_t pairhmm_batch_counts(const pairhmm_batch_t* batch, int64_t* pai
     std::string err;
     pairhmm_status_t s;
     try {
-        s = phmm::Engine::build_index(*batch, {{1 << 30, 32, 32, true}}, x, err);
+        s = phmm::Engine::build_index(*batch, {{1 << 30, 32, 32, true, false}}, x, err);
     } catch (...) {
         return PAIRHMM_ERR_OUT_OF_MEMORY;
     }
@@ -228,7 +228,10 @@ pairhmm_status_t pairhmm_set_tile_table(pairhmm_engine_t* h, const int32_t* max_
     if (!h || !max_len || !group || !regs || !multi_tile || n <= 0) return PAIRHMM_ERR_INVALID_ARGUMENT;
     return guarded(h, [&] {
         std::vector<phmm::TileRule> rules(n);
-        for (int i = 0; i < n; ++i) rules[i] = {max_len[i], group[i], regs[i], multi_tile[i] != 0};
+        for (int i = 0; i < n; ++i) {
+            if (multi_tile[i] < 0 || multi_tile[i] > 2) return PAIRHMM_ERR_INVALID_ARGUMENT;
+            rules[i] = {max_len[i], group[i], regs[i], multi_tile[i] == 1, multi_tile[i] == 2};
+        }
         return finish(h, h->engine->set_tile_table(rules));
     });
 }
@@ -243,7 +246,7 @@ pairhmm_status_t pairhmm_get_tile_table(pairhmm_engine_t* h, int32_t* max_len, i
         max_len[i] = r[i].max_len;
         group[i] = r[i].G;
         regs[i] = r[i].R;
-        multi_tile[i] = r[i].multi_tile ? 1 : 0;
+        multi_tile[i] = r[i].multi_tile ? 1 : (r[i].packed ? 2 : 0);
     }
     return PAIRHMM_OK;
 }

@@ -8,8 +8,9 @@
 //              haplotype starts at a multiple of 16 bytes and is padded with 4;
 //              the arena ends with kHapSlack bytes of 4 so a group may read a
 //              few words past the end of its haplotype.
-//   tasks      16-byte work items (read, hap, output slot), sorted by
-//              (length bucket, haplotype length descending).
+//   items      32-byte work items (one or two reads x one haplotype, output
+//              slots), sorted by (length bucket, haplotype length descending);
+//              the FP64 pass takes 16-byte single-pair tasks.
 #pragma once
 
 #include <cfloat>
@@ -48,6 +49,21 @@ struct Task {
 };
 static_assert(sizeof(Task) == 16, "Task must be 16 bytes");
 
+// Work item of the FP32 pass: a unit (one read, or two reads of the same
+// record and length bucket for the packed kernel) against one haplotype.
+struct Item {
+    int32_t read0;
+    int32_t read1;  // -1 when the unit holds one read
+    int32_t hap;
+    int32_t pad;
+    int64_t out0;   // output slot of (read0, hap)
+    int64_t out1;   // output slot of (read1, hap), -1 when absent
+};
+static_assert(sizeof(Item) == 32, "Item must be 32 bytes");
+
+struct DevView;
+__device__ __forceinline__ void append_rescue(const DevView& v, int cls, const Task& t);
+
 struct DevView {
     const uint32_t* read_pack;
     const int64_t* read_start;  // in positions, multiple of 4
@@ -75,6 +91,16 @@ constexpr int kFp64Classes = 5;
 constexpr int kFp64ClassMax[kFp64Classes - 1] = {64, 96, 128, 192};
 __host__ __device__ __forceinline__ int fp64_class(int L) {
     return L <= 64 ? 0 : L <= 96 ? 1 : L <= 128 ? 2 : L <= 192 ? 3 : 4;
+}
+
+// Appends a flagged pair to its FP64 class list.  The list pointer is picked
+// with constant indices: a run-time index into the kernel-parameter array would
+// copy the whole parameter block to local memory.
+__device__ __forceinline__ void append_rescue(const DevView& v, int cls, const Task& t) {
+    Task* dst = cls == 0 ? v.rescue[0] : cls == 1 ? v.rescue[1] : cls == 2 ? v.rescue[2]
+              : cls == 3 ? v.rescue[3] : v.rescue[4];
+    const unsigned long long slot = atomicAdd(v.rescue_count + cls, 1ull);
+    dst[slot] = t;
 }
 
 }  // namespace phmm

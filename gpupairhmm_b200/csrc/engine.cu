@@ -89,7 +89,7 @@ Engine::~Engine() {
                       &in_iq_, &in_dq_, &in_read_off_, &in_read_len_, &in_hap_bases_, &in_hap_off_, &in_hap_len_,
                       &read_record_, &read_local_, &rec_haps_, &rec_hap_base_, &rec_pair_base_, &read_start_,
                       &hap_start_, &read_pack_, &hap_code_, &hist_, &cursor_, &items_, &rescue_, &counters_,
-                      &sched_, &scores_, &scratch_, &lens_tmp_};
+                      &sched_, &scores_, &scratch_, &lens_tmp_, &unit_read0_, &unit_read1_, &unit_bucket_};
     for (DevBuf* b : bufs) b->release();
     if (pinned_) cudaFreeHost(pinned_);
     if (ev0_) cudaEventDestroy(ev0_);
@@ -152,7 +152,9 @@ pairhmm_status_t Engine::init() {
 pairhmm_status_t Engine::set_tile_table(const std::vector<TileRule>& rules) {
     if (rules.empty() || (int)rules.size() > kMaxBuckets) return fail(PAIRHMM_ERR_INVALID_ARGUMENT, "tile table size");
     for (size_t i = 0; i < rules.size(); ++i) {
-        if (!find_fp32_config(rules[i].G, rules[i].R, rules[i].multi_tile))
+        if (rules[i].packed && rules[i].multi_tile)
+            return fail(PAIRHMM_ERR_INVALID_ARGUMENT, "packed rules are single tile");
+        if (!find_fp32_config(rules[i].G, rules[i].R, rules[i].multi_tile, rules[i].packed))
             return fail(PAIRHMM_ERR_INVALID_ARGUMENT, "tile table names a configuration that is not compiled");
         if (i > 0 && rules[i].max_len <= rules[i - 1].max_len)
             return fail(PAIRHMM_ERR_INVALID_ARGUMENT, "tile table bounds must increase");
@@ -173,7 +175,7 @@ pairhmm_status_t Engine::upload_rules() {
     rule_cfg_.assign(nb, nullptr);
     std::vector<int32_t> maxlen(nb), rank(nb), per(nb), cfg(nb);
     for (int b = 0; b < nb; ++b) {
-        rule_cfg_[b] = find_fp32_config(rules_[b].G, rules_[b].R, rules_[b].multi_tile);
+        rule_cfg_[b] = find_fp32_config(rules_[b].G, rules_[b].R, rules_[b].multi_tile, rules_[b].packed);
         if (!rule_cfg_[b]) return fail(PAIRHMM_ERR_INVALID_ARGUMENT, "tile rule without compiled kernel");
         maxlen[b] = rules_[b].max_len;
         rank[b] = opts_.mode == PAIRHMM_MODE_PLAIN ? b : nb - 1 - b;
@@ -263,6 +265,47 @@ pairhmm_status_t Engine::build_index(const pairhmm_batch_t& b, const std::vector
         x.hap_start[h] = x.code_bytes;
         x.code_bytes += round_up(H, 16);
     }
+    // units: reads of a record in the same bucket, paired when the bucket's
+    // kernel is packed (order inside a record does not matter: output slots
+    // are per read)
+    x.bucket_items.assign(rules.size(), 0);
+    x.unit_read0.reserve(x.num_reads);
+    x.unit_read1.reserve(x.num_reads);
+    x.unit_bucket.reserve(x.num_reads);
+    {
+        std::vector<int32_t> pending(rules.size(), -1);
+        int64_t i = 0;
+        for (int64_t g = 0; g < b.num_records; ++g) {
+            const int64_t H = x.rec_haps[g];
+            std::vector<int> touched;
+            for (int32_t r = 0; r < b.reads_per_record[g]; ++r, ++i) {
+                const int bk = bucket_of_host(b.read_lengths[i], rules);
+                if (rules[bk].packed) {
+                    if (pending[bk] < 0) {
+                        pending[bk] = (int32_t)i;
+                        touched.push_back(bk);
+                        continue;
+                    }
+                    x.unit_read0.push_back(pending[bk]);
+                    x.unit_read1.push_back((int32_t)i);
+                    pending[bk] = -1;
+                } else {
+                    x.unit_read0.push_back((int32_t)i);
+                    x.unit_read1.push_back(-1);
+                }
+                x.unit_bucket.push_back(bk);
+                x.bucket_items[bk] += H;
+            }
+            for (int bk : touched)
+                if (pending[bk] >= 0) {
+                    x.unit_read0.push_back(pending[bk]);
+                    x.unit_read1.push_back(-1);
+                    x.unit_bucket.push_back(bk);
+                    x.bucket_items[bk] += H;
+                    pending[bk] = -1;
+                }
+        }
+    }
     // cells: sum over records of (sum L) * (sum H)  (gpuworker.cuh:495-520)
     {
         int64_t i = 0;
@@ -299,13 +342,16 @@ pairhmm_status_t Engine::ensure_buffers(const BatchIndex& x, bool host_inputs) {
     PHMM_CUDA(rec_hap_base_.ensure(8 * ng));
     PHMM_CUDA(rec_pair_base_.ensure(8 * ng));
     PHMM_CUDA(read_start_.ensure(8 * nr));
+    PHMM_CUDA(unit_read0_.ensure(4 * nr));
+    PHMM_CUDA(unit_read1_.ensure(4 * nr));
+    PHMM_CUDA(unit_bucket_.ensure(4 * nr));
     PHMM_CUDA(hap_start_.ensure(8 * nh));
     PHMM_CUDA(read_pack_.ensure(4 * (x.pack_positions + kReadSlackPos)));
     PHMM_CUDA(hap_code_.ensure(x.code_bytes + kHapSlack));
     const int64_t nbins = (int64_t)rules_.size() * (opts_.mode == PAIRHMM_MODE_PLAIN ? 1 : kHBins);
     PHMM_CUDA(hist_.ensure(4 * nbins));
     PHMM_CUDA(cursor_.ensure(8 * nbins));
-    PHMM_CUDA(items_.ensure(sizeof(Task) * np));
+    PHMM_CUDA(items_.ensure(sizeof(Item) * np));
     PHMM_CUDA(rescue_.ensure(sizeof(Task) * np));  // class lists laid out back to back
     return PAIRHMM_OK;
 }
@@ -320,6 +366,9 @@ pairhmm_status_t Engine::upload_index(const BatchIndex& x, cudaStream_t s) {
         {&rec_pair_base_, x.rec_pair_base.data(), 8 * x.rec_pair_base.size()},
         {&read_start_, x.read_start.data(), 8 * x.read_start.size()},
         {&hap_start_, x.hap_start.data(), 8 * x.hap_start.size()},
+        {&unit_read0_, x.unit_read0.data(), 4 * x.unit_read0.size()},
+        {&unit_read1_, x.unit_read1.data(), 4 * x.unit_read1.size()},
+        {&unit_bucket_, x.unit_bucket.data(), 4 * x.unit_bucket.size()},
     };
     size_t total = 0;
     for (const Piece& p : pieces) total += round_up((int64_t)p.bytes, 256);
@@ -346,7 +395,8 @@ pairhmm_status_t Engine::upload_index(const BatchIndex& x, cudaStream_t s) {
 }
 
 int64_t Engine::index_bytes(const BatchIndex& x) {
-    return 4 * (int64_t)(x.read_record.size() + x.read_local.size() + x.rec_haps.size()) +
+    return 4 * (int64_t)(x.read_record.size() + x.read_local.size() + x.rec_haps.size() + x.unit_read0.size() +
+                         x.unit_read1.size() + x.unit_bucket.size()) +
            8 * (int64_t)(x.rec_hap_base.size() + x.rec_pair_base.size() + x.read_start.size() + x.hap_start.size());
 }
 
@@ -393,21 +443,22 @@ pairhmm_status_t Engine::enqueue_pipeline(const pairhmm_batch_t& in, const Batch
     }
 
     BinArgs ba{};
-    ba.read_lengths = in.read_lengths;
     ba.hap_lengths = in.hap_lengths;
     ba.read_record = pa.read_record;
     ba.read_local = pa.read_local;
     ba.rec_haps = pa.rec_haps;
     ba.rec_hap_base = pa.rec_hap_base;
     ba.rec_pair_base = pa.rec_pair_base;
-    ba.num_reads = x.num_reads;
+    ba.unit_read0 = unit_read0_.as<int32_t>();
+    ba.unit_read1 = unit_read1_.as<int32_t>();
+    ba.unit_bucket = unit_bucket_.as<int32_t>();
+    ba.num_units = (int64_t)x.unit_read0.size();
     ba.nbuckets = nb;
     ba.hbins = plain ? 1 : kHBins;
-    ba.bucket_max_len = rules_maxlen_.as<int32_t>();
     ba.bucket_rank = rules_rank_.as<int32_t>();
     ba.hist = hist_.as<unsigned int>();
     ba.cursor = cursor_.as<unsigned long long>();
-    ba.items = items_.as<Task>();
+    ba.items = items_.as<Item>();
     if (stage == 0) {
     PHMM_CUDA(launch_binning(ba, prep_grid, s, per_task_.as<int>(), config_.as<int>(), sched_.as<Schedule>(), nb));
     launches_ += 4;
@@ -438,11 +489,11 @@ pairhmm_status_t Engine::enqueue_pipeline(const pairhmm_batch_t& in, const Batch
     if (stage == 1) {
     for (int rank = 0; rank < nb; ++rank) {
         const int b = plain ? rank : nb - 1 - rank;
-        if (x.bucket_pairs[b] == 0) continue;
+        if (x.bucket_items[b] == 0) continue;
         const ConfigInfo* c = rule_cfg_[b];
         Fp32LaunchArgs la{};
         la.view = v;
-        la.items = items_.as<Task>();
+        la.items = items_.as<Item>();
         la.sched = sched_.as<Schedule>();
         la.rank = rank;
         la.persistent = plan.persistent[b];
@@ -484,9 +535,9 @@ Engine::Plan Engine::make_plan(const BatchIndex& x) const {
     p.persistent.assign(nb, 1);
     int64_t scratch = 0;
     for (int b = 0; b < nb; ++b) {
-        if (x.bucket_pairs[b] == 0) continue;
+        if (x.bucket_items[b] == 0) continue;
         const ConfigInfo* c = rule_cfg_[b];
-        const int64_t tasks = (x.bucket_pairs[b] + c->per_warp() - 1) / c->per_warp();
+        const int64_t tasks = (x.bucket_items[b] + c->per_warp() - 1) / c->per_warp();
         const int64_t need_blocks = (tasks + kWarpsPerBlock - 1) / kWarpsPerBlock;
         int64_t grid = plain ? need_blocks : std::min<int64_t>(persistent_grid(c->kernel, c->smem_bytes), need_blocks);
         if (c->multi_tile) {

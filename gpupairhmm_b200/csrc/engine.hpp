@@ -19,6 +19,7 @@ struct TileRule {
     int G;
     int R;
     bool multi_tile;
+    bool packed = false;  // two reads of a record per group, packed FP32 (single tile)
 };
 
 // Per-batch index derived on the host from the record structure.
@@ -31,6 +32,8 @@ struct BatchIndex {
     std::vector<int32_t> read_record, read_local, rec_haps;
     std::vector<int64_t> rec_hap_base, rec_pair_base, read_start, hap_start;
     std::vector<int64_t> bucket_pairs;              // by bucket index
+    std::vector<int64_t> bucket_items;              // work items (unit x haplotype) by bucket
+    std::vector<int32_t> unit_read0, unit_read1, unit_bucket;  // units: 1 or 2 reads of a record
     int64_t class_pairs[kFp64Classes] = {};         // by FP64 length class (fp64_class)
     int64_t multi_tile_pairs = 0;
 };
@@ -107,6 +110,7 @@ private:
     DevBuf in_read_bases_, in_bq_, in_iq_, in_dq_, in_read_off_, in_read_len_;
     DevBuf in_hap_bases_, in_hap_off_, in_hap_len_;
     DevBuf read_record_, read_local_, rec_haps_, rec_hap_base_, rec_pair_base_, read_start_, hap_start_;
+    DevBuf unit_read0_, unit_read1_, unit_bucket_;
     DevBuf read_pack_, hap_code_, hist_, cursor_, items_, rescue_, counters_, sched_, scores_, scratch_;
     DevBuf lens_tmp_;
     // pinned staging for the index upload

@@ -16,6 +16,9 @@ void register_fp32_g32(std::vector<ConfigInfo>& out) {
     out.push_back(make_fp32_config<32, 24, true>());
     out.push_back(make_fp32_config<32, 28, true>());
     out.push_back(make_fp32_config<32, 32, true>());
+    out.push_back(make_fp32_config<32, 8, false, true>());
+    out.push_back(make_fp32_config<32, 12, false, true>());
+    out.push_back(make_fp32_config<32, 16, false, true>());
 }
 
 }  // namespace phmm

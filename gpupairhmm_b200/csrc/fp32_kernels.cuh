@@ -1,8 +1,11 @@
 // __global__ wrapper around Fp32Wavefront and its registration.
 #pragma once
 
+#include <type_traits>
+
 #include "kernels.hpp"
 #include "wavefront_fp32.cuh"
+#include "wavefront_fp32x2.cuh"
 
 namespace phmm {
 
@@ -11,11 +14,15 @@ namespace phmm {
 // longest first, so this is longest-processing-time-first scheduling).
 // persistent = 0: warp w of the grid runs task w once (one launch per
 // partition, the reference's execution form).
-template <int G, int R, bool MT>
+template <int G, int R, bool MT, bool PK>
+using WavefrontOf = typename std::conditional<PK, Fp32x2Wavefront<G, R>, Fp32Wavefront<G, R, MT>>::type;
+
+template <int G, int R, bool MT, bool PK>
 __global__ void __launch_bounds__(kBlockThreads)
-fp32_bucket_kernel(DevView v, const Task* __restrict__ items, const Schedule* __restrict__ s, int rank,
+fp32_bucket_kernel(DevView v, const Item* __restrict__ items, const Schedule* __restrict__ s, int rank,
                    int persistent, unsigned long long* counter, float4* scratch, int64_t rows) {
-    using W = Fp32Wavefront<G, R, MT>;
+    static_assert(!(MT && PK), "the packed kernel is single tile");
+    using W = WavefrontOf<G, R, MT, PK>;
     extern __shared__ float4 smem[];
     float* ph = reinterpret_cast<float*>(smem);
     const int warp = threadIdx.x >> 5;
@@ -41,31 +48,33 @@ fp32_bucket_kernel(DevView v, const Task* __restrict__ items, const Schedule* __
         if (tsk >= ntasks) break;
         const long long first = ib + tsk * per;
         const int n = (int)((ie - first) < per ? (ie - first) : per);
-        W::run(v, items + first, n, wtab, ph, wscratch, rows);
+        if constexpr (PK) W::run(v, items + first, n, wtab, ph);
+        else W::run(v, items + first, n, wtab, ph, wscratch, rows);
         if (!persistent) break;
     }
 }
 
-template <int G, int R, bool MT>
+template <int G, int R, bool MT, bool PK>
 cudaError_t launch_fp32_bucket(const Fp32LaunchArgs& a) {
-    using W = Fp32Wavefront<G, R, MT>;
+    using W = WavefrontOf<G, R, MT, PK>;
     const size_t smem = (32 + (size_t)kWarpsPerBlock * W::kTableFloat4) * sizeof(float4);
-    fp32_bucket_kernel<G, R, MT><<<a.grid, kBlockThreads, smem, a.stream>>>(
+    fp32_bucket_kernel<G, R, MT, PK><<<a.grid, kBlockThreads, smem, a.stream>>>(
         a.view, a.items, a.sched, a.rank, a.persistent, a.counter, static_cast<float4*>(a.scratch), a.rows);
     return cudaGetLastError();
 }
 
-template <int G, int R, bool MT>
+template <int G, int R, bool MT, bool PK = false>
 ConfigInfo make_fp32_config() {
-    using W = Fp32Wavefront<G, R, MT>;
+    using W = WavefrontOf<G, R, MT, PK>;
     ConfigInfo c{};
     c.G = G;
     c.R = R;
     c.multi_tile = MT;
+    c.packed = PK;
     c.smem_bytes = (32 + (size_t)kWarpsPerBlock * W::kTableFloat4) * sizeof(float4);
     c.scratch_bytes_per_row = MT ? (size_t)W::NG * 2 * sizeof(float4) : 0;
-    c.kernel = reinterpret_cast<const void*>(&fp32_bucket_kernel<G, R, MT>);
-    c.launch = &launch_fp32_bucket<G, R, MT>;
+    c.kernel = reinterpret_cast<const void*>(&fp32_bucket_kernel<G, R, MT, PK>);
+    c.launch = &launch_fp32_bucket<G, R, MT, PK>;
     return c;
 }
 

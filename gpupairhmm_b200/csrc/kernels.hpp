@@ -17,7 +17,7 @@ constexpr int kWarpsPerBlock = kBlockThreads / 32;
 
 struct Fp32LaunchArgs {
     DevView view;
-    const Task* items;
+    const Item* items;
     const Schedule* sched;
     int rank;                       // bucket rank this launch serves
     int persistent;                 // 1: warps loop on an atomic task counter
@@ -44,8 +44,9 @@ struct ConfigInfo {
     int G;
     int R;
     bool multi_tile;
+    bool packed;                     // two reads per group with packed FP32 (single tile)
     int tile() const { return G * R; }
-    int per_warp() const { return 32 / G; }
+    int per_warp() const { return 32 / G; }   // items per warp task
     size_t smem_bytes;               // dynamic shared memory per CTA
     size_t scratch_bytes_per_row;    // per warp, per border row (both buffers)
     const void* kernel;
@@ -54,7 +55,7 @@ struct ConfigInfo {
 
 // All compiled FP32 configurations.
 const std::vector<ConfigInfo>& fp32_configs();
-const ConfigInfo* find_fp32_config(int G, int R, bool multi_tile);
+const ConfigInfo* find_fp32_config(int G, int R, bool multi_tile, bool packed = false);
 
 // FP64 pass, one kernel per length class: (G, R) = (8, 8), (16, 8) single
 // tile and (32, 8) multi-tile.

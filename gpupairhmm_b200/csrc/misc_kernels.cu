@@ -27,9 +27,9 @@ const std::vector<ConfigInfo>& fp32_configs() {
     return all;
 }
 
-const ConfigInfo* find_fp32_config(int G, int R, bool multi_tile) {
+const ConfigInfo* find_fp32_config(int G, int R, bool multi_tile, bool packed) {
     for (const auto& c : fp32_configs())
-        if (c.G == G && c.R == R && c.multi_tile == multi_tile) return &c;
+        if (c.G == G && c.R == R && c.multi_tile == multi_tile && c.packed == packed) return &c;
     return nullptr;
 }
 

@@ -1,10 +1,11 @@
 // Batch preparation kernels: pack reads and haplotypes into the HBM layout
 // of device_common.cuh, then build the sorted work list.
 //
-// Work list: every pair gets a bin  (bucket rank, 4095 - min(H, 4095))  so that
-// an exclusive scan over bins followed by an atomic scatter sorts the pairs by
-// tile bucket (largest tiles first) and, inside a bucket, by haplotype length
-// descending.  Warps of the persistent kernel then take consecutive items, so
+// Work list: every item (a unit of one or two reads of a record, placed in a
+// length bucket by the host, against one haplotype) gets a bin
+// (bucket rank, 4095 - min(H, 4095)) so that an exclusive scan over bins
+// followed by an atomic scatter sorts the items by tile bucket (largest tiles
+// first) and, inside a bucket, by haplotype length descending.  Warps of the persistent kernel then take consecutive items, so
 // the groups of a warp have nearly equal haplotype lengths (little idle work)
 // and the longest pairs start first (short tail).  The order of pairs with the
 // same bin is not deterministic; each pair still writes its own output slot,
@@ -87,33 +88,27 @@ __global__ void pack_haps_kernel(PrepArgs a) {
 #endif  // PHMM_PREP_KERNELS_IMPL
 
 struct BinArgs {
-    const int32_t* read_lengths;
     const int32_t* hap_lengths;
     const int32_t* read_record;
     const int32_t* read_local;
     const int32_t* rec_haps;
     const int64_t* rec_hap_base;
     const int64_t* rec_pair_base;
-    int64_t num_reads;
+    const int32_t* unit_read0;      // [num_units]
+    const int32_t* unit_read1;      // [num_units], -1 for a one-read unit
+    const int32_t* unit_bucket;     // [num_units]
+    int64_t num_units;
     int nbuckets;
     int hbins;                      // kHBins (engine) or 1 (plain)
-    const int32_t* bucket_max_len;  // [nbuckets] inclusive upper bound on L, ascending
     const int32_t* bucket_rank;     // [nbuckets] bin-major position of each bucket
     unsigned int* hist;             // [nbuckets * hbins]
     unsigned long long* cursor;     // [nbuckets * hbins] scatter positions
-    Task* items;
+    Item* items;
 };
 
-__device__ __forceinline__ int bucket_of(int L, const int32_t* bmax, int nb) {
-    int b = 0;
-    while (b < nb - 1 && L > bmax[b]) ++b;
-    return b;
-}
-
-__device__ __forceinline__ int bin_of(const BinArgs& a, int L, int H) {
-    const int b = bucket_of(L, a.bucket_max_len, a.nbuckets);
+__device__ __forceinline__ int bin_of(const BinArgs& a, int bucket, int H) {
     const int hc = a.hbins > 1 ? (a.hbins - 1 - (H < a.hbins - 1 ? H : a.hbins - 1)) : 0;
-    return a.bucket_rank[b] * a.hbins + hc;
+    return a.bucket_rank[bucket] * a.hbins + hc;
 }
 
 #ifdef PHMM_PREP_KERNELS_IMPL
@@ -130,35 +125,36 @@ __device__ __forceinline__ T aggregated_add(T* counter, unsigned key) {
     return base + (T)__popc(peers & ((1u << lane) - 1u));
 }
 
-// thread per read: histogram of (bucket, H class)
+// thread per unit: histogram of (bucket, H class)
 __global__ void bin_count_kernel(BinArgs a) {
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < a.num_reads;
-         i += (int64_t)gridDim.x * blockDim.x) {
-        const int L = a.read_lengths[i];
-        const int g = a.read_record[i];
+    for (int64_t u = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; u < a.num_units;
+         u += (int64_t)gridDim.x * blockDim.x) {
+        const int g = a.read_record[a.unit_read0[u]];
         const int nh = a.rec_haps[g];
         const int64_t hb = a.rec_hap_base[g];
+        const int b = a.unit_bucket[u];
         for (int h = 0; h < nh; ++h) {
-            const int bin = bin_of(a, L, a.hap_lengths[hb + h]);
+            const int bin = bin_of(a, b, a.hap_lengths[hb + h]);
             aggregated_add(&a.hist[bin], (unsigned)bin);
         }
     }
 }
 
-
-// thread per read: scatter items into their sorted slots
+// thread per unit: scatter items into their sorted slots
 __global__ void bin_scatter_kernel(BinArgs a) {
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < a.num_reads;
-         i += (int64_t)gridDim.x * blockDim.x) {
-        const int L = a.read_lengths[i];
-        const int g = a.read_record[i];
+    for (int64_t u = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; u < a.num_units;
+         u += (int64_t)gridDim.x * blockDim.x) {
+        const int r0 = a.unit_read0[u], r1 = a.unit_read1[u];
+        const int g = a.read_record[r0];
         const int nh = a.rec_haps[g];
         const int64_t hb = a.rec_hap_base[g];
-        const int64_t ob = a.rec_pair_base[g] + (int64_t)a.read_local[i] * nh;
+        const int b = a.unit_bucket[u];
+        const int64_t ob0 = a.rec_pair_base[g] + (int64_t)a.read_local[r0] * nh;
+        const int64_t ob1 = r1 >= 0 ? a.rec_pair_base[g] + (int64_t)a.read_local[r1] * nh : -1;
         for (int h = 0; h < nh; ++h) {
-            const int bin = bin_of(a, L, a.hap_lengths[hb + h]);
+            const int bin = bin_of(a, b, a.hap_lengths[hb + h]);
             const unsigned long long pos = aggregated_add(&a.cursor[bin], (unsigned)bin);
-            a.items[pos] = Task{(int32_t)i, (int32_t)(hb + h), ob + h};
+            a.items[pos] = Item{r0, r1, (int32_t)(hb + h), 0, ob0 + h, r1 >= 0 ? ob1 + h : -1};
         }
     }
 }

@@ -54,16 +54,17 @@ struct Fp32Wavefront {
     static constexpr int Q = R / 4;     // float4 per thread per table row
     static constexpr int kTableFloat4 = 5 * Q * 32;  // per warp
 
-    // tasks: the warp's ntask (<= NG) work items.  wtab: this warp's table
+    // items: the warp's ntask (<= NG) work items (read1 unused).  wtab: this warp's table
     // (kTableFloat4 float4).  ph: 128-entry probability table (shared).
     // scratch: this warp's border storage, NG groups x 2 buffers x rows float4.
-    __device__ static void run(const DevView& v, const Task* tasks, int ntask, float4* wtab,
+    __device__ static void run(const DevView& v, const Item* items, int ntask, float4* wtab,
                                const float* ph, float4* scratch, int64_t rows) {
         const int lane = threadIdx.x & 31;
         const int grp = lane / G;
         const int t = lane - grp * G;
         const bool active = grp < ntask;
-        const Task task = tasks[active ? grp : 0];
+        const Item it = items[active ? grp : 0];
+        const Task task{it.read0, it.hap, it.out0};  // units of this kernel hold one read
         const int L = v.read_len[task.read];
         const int H = v.hap_len[task.hap];
         const bool valid = active && L >= 1 && H >= 1;
@@ -264,9 +265,7 @@ struct Fp32Wavefront {
             const float res = log10f(acc) - (log10f(kScale) + log10f(kBeta));
             v.scores[task.out] = res;
             if (degenerate || (v.rescue_enabled && !(acc >= rescue_threshold(L, H) && acc <= FLT_MAX))) {
-                const int cls = fp64_class(L);
-                const unsigned long long slot = atomicAdd(v.rescue_count + cls, 1ull);
-                v.rescue[cls][slot] = task;
+                append_rescue(v, fp64_class(L), task);
             }
         }
     }

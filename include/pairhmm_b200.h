@@ -152,12 +152,14 @@ pairhmm_status_t pairhmm_region_latency_ms(pairhmm_engine_t* engine, uint64_t ti
 
 /*
  * Tile table: reads of length in (max_len[i-1], max_len[i]] run with groups of
- * group[i] lanes holding regs[i] read positions each (tile = group*regs), as
- * one tile or, when multi_tile[i] != 0, as several.  This is the run-time form
- * of the reference's compile-time tuning tables (tuningconfigs.hpp:33-269) and
- * of its partition rule "first tile size >= read length"
- * (utility_kernels.cuh:45-57).  Only compiled (group, regs) pairs are accepted;
- * the last entry must be multi-tile.
+ * group[i] lanes holding regs[i] read positions each (tile = group*regs).
+ * kind[i] (the `multi_tile` argument): 0 = one tile, 1 = several tiles
+ * (reads longer than the tile), 2 = one tile with two reads of a record per
+ * group in packed FP32 arithmetic.  This is the run-time form of the
+ * reference's compile-time tuning tables (tuningconfigs.hpp:33-269) and of its
+ * partition rule "first tile size >= read length" (utility_kernels.cuh:45-57).
+ * Only compiled (group, regs, kind) triples are accepted; the last entry must
+ * be multi-tile.
  */
 pairhmm_status_t pairhmm_set_tile_table(pairhmm_engine_t* engine, const int32_t* max_len, const int32_t* group,
                                         const int32_t* regs, const int32_t* multi_tile, int32_t n);

@@ -213,6 +213,32 @@ def test_pinned_host_inputs(engine):
     np.testing.assert_array_equal(engine.compute(b.pin()), engine.compute(b))
 
 
+PACKED_TABLE = [(32, 4, 8, 2), (48, 4, 12, 2), (64, 4, 16, 2), (96, 8, 12, 2), (128, 8, 16, 2),
+                (192, 16, 12, 2), (256, 16, 16, 2), (384, 32, 12, 2), (512, 32, 16, 2), (1024, 32, 32, 0),
+                (1 << 30, 32, 32, 1)]
+
+
+def test_packed_kernel_matches_oracle():
+    """Two reads per group in packed FP32: odd read counts (one-read units),
+    reads of different lengths in one unit, every packed tile size."""
+    e = g.Engine()
+    e.set_tile_table(PACKED_TABLE)
+    rng = np.random.default_rng(31)
+    recs = []
+    for L in [1, 5, 17, 31, 33, 47, 64, 65, 95, 97, 128, 129, 191, 193, 256, 257, 383, 385, 511, 512]:
+        H = int(rng.integers(1, 3 * L + 50))
+        recs.append(_record(rng, L, H, n_reads=1 + L % 3, n_haps=1 + L % 4))
+    b = synth.concat([_soa(recs), synth.config0(seed=2, records=3), synth.config2(seed=3, regions=1, reads=7, haps=3)])
+    got = e.compute(b)
+    assert_log10_close(got, oracle.batch_log10(b), what="packed")
+    # scalar and packed single-tile kernels agree within the tolerance
+    e2 = g.Engine()
+    e2.set_tile_table([(r[0], r[1], r[2], 0 if r[3] == 2 else r[3]) for r in PACKED_TABLE])
+    assert_log10_close(got, e2.compute(b), what="packed vs scalar")
+    e.close()
+    e2.close()
+
+
 def test_tile_table_round_trip_and_validation():
     e = g.Engine()
     t = e.tile_table()
@@ -220,10 +246,13 @@ def test_tile_table_round_trip_and_validation():
     b = synth.config1(seed=20, regions=10)
     base = e.compute(b)
     # a coarser table (different tiles) gives the same results within tolerance
-    e.set_tile_table([(128, 8, 16, False), (256, 16, 16, False), (512, 32, 16, False), (1 << 30, 32, 32, True)])
+    e.set_tile_table([(128, 8, 16, 0), (256, 16, 16, 2), (512, 32, 16, 0), (1 << 30, 32, 32, 1)])
+    assert e.tile_table()[1] == (256, 16, 16, 2)
     assert_log10_close(e.compute(b), base, what="alt table")
     with pytest.raises(g.PairHMMError):
         e.set_tile_table([(128, 4, 8, False), (1 << 30, 32, 32, True)])  # 128 > 4*8
     with pytest.raises(g.PairHMMError):
         e.set_tile_table([(128, 4, 32, False)])  # last rule must be multi-tile
+    with pytest.raises(g.PairHMMError):
+        e.set_tile_table([(128, 4, 32, 2), (1 << 30, 32, 32, 1)])  # no packed 4x32 kernel
     e.close()
