@@ -35,6 +35,7 @@ MODE_PLAIN = 1
 STATUS = {
     0: "ok", 1: "invalid argument", 2: "CUDA error", 3: "out of memory", 4: "region exceeds the device budget",
     5: "unknown ticket", 6: "timed out", 7: "unsupported", 8: "busy",
+    9: "haplotype length above the no-alloc limit of 16384",
 }
 
 
@@ -113,6 +114,8 @@ _SIGNATURES = {
     "pairhmm_records_view": (ctypes.c_int, [_P, _P, _P]),
     "pairhmm_records_format": (ctypes.c_int, [_P, _P, _P, ctypes.c_int64, _P]),
     "pairhmm_records_free": (None, [_P]),
+    "pairhmm_forward_pairs_noalloc": (ctypes.c_int, [ctypes.c_int32] + [_P] * 6 + [ctypes.c_int64, ctypes.c_int32,
+                                                                                  _P, _P]),
 }
 
 _lib = None
@@ -357,6 +360,20 @@ def probe_fp32_peak(device: int = 0, milliseconds: int = 50) -> float:
     v = ctypes.c_double()
     _check(lib().pairhmm_probe_fp32_peak(device, milliseconds, ctypes.byref(v)))
     return float(v.value)
+
+
+PAIR_DTYPE = np.dtype([("read_offset", "<i8"), ("hap_offset", "<i8"), ("read_length", "<i4"),
+                       ("hap_length", "<i4")])
+
+
+def forward_pairs_noalloc(device: int, read_bases, base_quals, ins_quals, del_quals, hap_bases, pairs,
+                          num_pairs: int, max_hap_length: int, scores, stream=None) -> None:
+    """Allocation-free forward over a flat pair list (all arguments device
+    tensors, `pairs` laid out as PAIR_DTYPE).  See pairhmm_forward_pairs_noalloc."""
+    st = None if stream is None else ctypes.c_void_p(stream.cuda_stream)
+    _check(lib().pairhmm_forward_pairs_noalloc(device, _ptr(read_bases), _ptr(base_quals), _ptr(ins_quals),
+                                               _ptr(del_quals), _ptr(hap_bases), _ptr(pairs), num_pairs,
+                                               max_hap_length, _ptr(scores), st))
 
 
 def version() -> str:

@@ -158,6 +158,7 @@ const char* pairhmm_status_string(pairhmm_status_t s) {
         case PAIRHMM_ERR_TIMEOUT: return "timed out";
         case PAIRHMM_ERR_UNSUPPORTED: return "unsupported";
         case PAIRHMM_ERR_BUSY: return "busy";
+        case PAIRHMM_ERR_LIMIT: return "haplotype length above the no-alloc limit of 16384";
     }
     return "unknown status";
 }

@@ -48,7 +48,8 @@ typedef enum pairhmm_status {
     PAIRHMM_ERR_NOT_FOUND = 5,        /* serving: unknown ticket */
     PAIRHMM_ERR_TIMEOUT = 6,          /* a bounded device wait gave up */
     PAIRHMM_ERR_UNSUPPORTED = 7,      /* no sm_100 device, or feature not built */
-    PAIRHMM_ERR_BUSY = 8              /* serving: queue full, retry after draining */
+    PAIRHMM_ERR_BUSY = 8,             /* serving: queue full, retry after draining */
+    PAIRHMM_ERR_LIMIT = 9             /* no-alloc forward: max_hap_length above 16384 */
 } pairhmm_status_t;
 
 /*
@@ -189,6 +190,37 @@ pairhmm_status_t pairhmm_records_view(const pairhmm_records_t* records, pairhmm_
 pairhmm_status_t pairhmm_records_format(const pairhmm_records_t* records, const float* scores, char* buf,
                                         int64_t capacity, int64_t* length);
 void pairhmm_records_free(pairhmm_records_t* records);
+
+/*
+ * No counterpart in the reference.  Allocation-free forward for callers that
+ * cannot allocate device memory (a host that owns every device allocation, or
+ * a context where cudaMalloc/cudaFree must not run because they synchronise
+ * the device).  All arrays are the caller's device memory: the byte arrays
+ * with the same meaning as in pairhmm_batch_t, `pairs` a flat list (offsets
+ * into those arrays and lengths), `scores` one float per pair.  Work is
+ * ordered on `stream` (a cudaStream_t, NULL = legacy default); the call does
+ * not wait for it.  Nothing is allocated: the kernel's only scratch (borders
+ * between 512-position read tiles) is a 64 MiB statically allocated device
+ * array that every GPU loading the library keeps until exit.  Limits:
+ * max_hap_length in [1, 16384] (above: PAIRHMM_ERR_LIMIT, nothing launched)
+ * and every pair's hap_length <= max_hap_length (a longer pair, or an empty
+ * read or haplotype, gets NaN); any read length.  FP32 only: pairs whose FP32
+ * result underflows are not recomputed in FP64.  The first call on a device
+ * sets it up (scratch address, probability table); make that first call
+ * before any stream capture.  All calls share the scratch: calls that overlap
+ * on the GPU race and must be serialised by the caller.
+ */
+typedef struct pairhmm_pair {
+    int64_t read_offset;
+    int64_t hap_offset;
+    int32_t read_length;
+    int32_t hap_length;
+} pairhmm_pair_t;
+pairhmm_status_t pairhmm_forward_pairs_noalloc(int32_t device, const uint8_t* read_bases,
+                                               const uint8_t* base_quals, const uint8_t* ins_quals,
+                                               const uint8_t* del_quals, const uint8_t* hap_bases,
+                                               const pairhmm_pair_t* pairs, int64_t num_pairs,
+                                               int32_t max_hap_length, float* scores, void* stream);
 
 const char* pairhmm_status_string(pairhmm_status_t status);
 /* Message of the last failing call on this engine (empty when none). */
