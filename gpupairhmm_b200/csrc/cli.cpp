@@ -132,7 +132,7 @@ void gpu_thread(const Options& o, Queue<PipelineData*>* in, Queue<PipelineData*>
             *cells_total += s.cells;
             if (o.verbose)
                 std::cout << "chunk: " << s.pairs << " pairs, " << s.rescued << " rescued, " << s.device_ms
-                          << " ms device\n";
+                          << " ms device, " << s.total_ms << " ms in the call\n";
             g = g1;
             read0 += reads;
             hap0 += haps;

@@ -15,6 +15,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstring>
+#include <thread>
 
 #include "engine.hpp"
 
@@ -91,7 +92,6 @@ Engine::~Engine() {
                       &hap_start_, &read_pack_, &hap_code_, &hist_, &cursor_, &items_, &rescue_, &counters_,
                       &sched_, &scores_, &scratch_, &lens_tmp_, &unit_read0_, &unit_read1_, &unit_bucket_};
     for (DevBuf* b : bufs) b->release();
-    if (pinned_) cudaFreeHost(pinned_);
     if (ev0_) cudaEventDestroy(ev0_);
     if (ev1_) cudaEventDestroy(ev1_);
     if (ev_prep_) cudaEventDestroy(ev_prep_);
@@ -197,7 +197,19 @@ pairhmm_status_t Engine::upload_rules() {
 
 pairhmm_status_t Engine::build_index(const pairhmm_batch_t& b, const std::vector<TileRule>& rules, BatchIndex& x,
                                      std::string& err) {
-    x = BatchIndex{};
+    // Scalars reset; vectors keep their storage between calls (an engine
+    // reuses one index, so a batch of the same size touches no fresh pages).
+    x.num_records = x.num_reads = x.num_haps = x.num_pairs = x.cells = 0;
+    x.max_read_len = x.max_hap_len = 0;
+    x.read_bytes = x.hap_bytes = x.read_min = x.hap_min = 0;
+    x.pack_positions = x.code_bytes = 0;
+    x.multi_tile_pairs = 0;
+    for (int64_t& c : x.class_pairs) c = 0;
+    x.unit_read0.clear();
+    x.unit_read1.clear();
+    x.unit_bucket.clear();
+    x.bucket_pairs.assign(rules.size(), 0);
+    x.bucket_items.assign(rules.size(), 0);
     if (b.num_records < 0) { err = "num_records < 0"; return PAIRHMM_ERR_INVALID_ARGUMENT; }
     x.num_records = b.num_records;
     if (b.num_records == 0) return PAIRHMM_OK;
@@ -227,95 +239,170 @@ pairhmm_status_t Engine::build_index(const pairhmm_batch_t& b, const std::vector
     x.read_local.resize(x.num_reads);
     x.read_start.resize(x.num_reads);
     x.hap_start.resize(x.num_haps);
-    x.bucket_pairs.assign(rules.size(), 0);
-    {
-        int64_t i = 0;
-        for (int64_t g = 0; g < b.num_records; ++g)
-            for (int32_t r = 0; r < b.reads_per_record[g]; ++r, ++i) {
-                x.read_record[i] = (int32_t)g;
-                x.read_local[i] = r;
-            }
-    }
-    for (int64_t i = 0; i < x.num_reads; ++i) {
-        const int32_t L = b.read_lengths[i];
-        if (L < 1) { err = "read length < 1"; return PAIRHMM_ERR_INVALID_ARGUMENT; }
-        if (b.read_offsets) {
-            if (b.read_offsets[i] < 0) { err = "negative read offset"; return PAIRHMM_ERR_INVALID_ARGUMENT; }
-            x.read_bytes = std::max<int64_t>(x.read_bytes, b.read_offsets[i] + L);
-            x.read_min = i == 0 ? b.read_offsets[i] : std::min<int64_t>(x.read_min, b.read_offsets[i]);
-        }
-        x.max_read_len = std::max(x.max_read_len, L);
-        x.read_start[i] = x.pack_positions;
-        x.pack_positions += round_up(L, 4);
-        const int bk = bucket_of_host(L, rules);
-        const int64_t H = x.rec_haps[x.read_record[i]];
-        x.bucket_pairs[bk] += H;
-        x.class_pairs[fp64_class(L)] += H;
-        if (rules[bk].multi_tile) x.multi_tile_pairs += H;
-    }
-    for (int64_t h = 0; h < x.num_haps; ++h) {
-        const int32_t H = b.hap_lengths[h];
-        if (H < 1) { err = "haplotype length < 1"; return PAIRHMM_ERR_INVALID_ARGUMENT; }
-        if (b.hap_offsets) {
-            if (b.hap_offsets[h] < 0) { err = "negative haplotype offset"; return PAIRHMM_ERR_INVALID_ARGUMENT; }
-            x.hap_bytes = std::max<int64_t>(x.hap_bytes, b.hap_offsets[h] + H);
-            x.hap_min = h == 0 ? b.hap_offsets[h] : std::min<int64_t>(x.hap_min, b.hap_offsets[h]);
-        }
-        x.max_hap_len = std::max(x.max_hap_len, H);
-        x.hap_start[h] = x.code_bytes;
-        x.code_bytes += round_up(H, 16);
-    }
-    // units: reads of a record in the same bucket, paired when the bucket's
-    // kernel is packed (order inside a record does not matter: output slots
-    // are per read)
-    x.bucket_items.assign(rules.size(), 0);
     x.unit_read0.reserve(x.num_reads);
     x.unit_read1.reserve(x.num_reads);
     x.unit_bucket.reserve(x.num_reads);
+
+    // bucket of every read length up to the longest finite rule, by table
+    const int nb = (int)rules.size();
+    int lut_max = 0;
+    for (const TileRule& r : rules)
+        if (r.max_len < (1 << 20)) lut_max = std::max(lut_max, r.max_len);
+    std::vector<uint8_t> lut((size_t)lut_max + 1);
+    for (int L = 0, bk = 0; L <= lut_max; ++L) {
+        while (bk < nb - 1 && L > rules[bk].max_len) ++bk;
+        lut[L] = (uint8_t)bk;
+    }
+    std::vector<uint8_t> packed(nb), multi(nb);
+    for (int k = 0; k < nb; ++k) {
+        packed[k] = rules[k].packed;
+        multi[k] = rules[k].multi_tile;
+    }
+
+    // haplotypes: extents, packed starts, per-record length sums
+    std::vector<int64_t> rec_hap_sum(b.num_records);
     {
-        std::vector<int32_t> pending(rules.size(), -1);
-        int64_t i = 0;
+        int64_t h = 0;
         for (int64_t g = 0; g < b.num_records; ++g) {
-            const int64_t H = x.rec_haps[g];
-            std::vector<int> touched;
-            for (int32_t r = 0; r < b.reads_per_record[g]; ++r, ++i) {
-                const int bk = bucket_of_host(b.read_lengths[i], rules);
-                if (rules[bk].packed) {
-                    if (pending[bk] < 0) {
-                        pending[bk] = (int32_t)i;
-                        touched.push_back(bk);
-                        continue;
-                    }
-                    x.unit_read0.push_back(pending[bk]);
-                    x.unit_read1.push_back((int32_t)i);
-                    pending[bk] = -1;
-                } else {
-                    x.unit_read0.push_back((int32_t)i);
-                    x.unit_read1.push_back(-1);
+            int64_t sh = 0;
+            for (int32_t k = 0; k < x.rec_haps[g]; ++k, ++h) {
+                const int32_t H = b.hap_lengths[h];
+                if (H < 1) { err = "haplotype length < 1"; return PAIRHMM_ERR_INVALID_ARGUMENT; }
+                if (b.hap_offsets) {
+                    const int64_t o = b.hap_offsets[h];
+                    if (o < 0) { err = "negative haplotype offset"; return PAIRHMM_ERR_INVALID_ARGUMENT; }
+                    x.hap_bytes = std::max<int64_t>(x.hap_bytes, o + H);
+                    x.hap_min = h == 0 ? o : std::min<int64_t>(x.hap_min, o);
                 }
+                x.max_hap_len = std::max(x.max_hap_len, H);
+                x.hap_start[h] = x.code_bytes;
+                x.code_bytes += round_up(H, 16);
+                sh += H;
+            }
+            rec_hap_sum[g] = sh;
+        }
+    }
+
+    // reads, one record at a time: record/local index, packed start, bucket
+    // counts, and units -- reads of a record in the same bucket, paired when
+    // the bucket's kernel is packed (order inside a record does not matter:
+    // output slots are per read); cells = sum over records of
+    // (sum L) * (sum H) (gpuworker.cuh:495-520)
+    std::vector<int32_t> pending(nb, -1);
+    std::vector<int> touched;
+    touched.reserve(nb);
+    int64_t i = 0;
+    for (int64_t g = 0; g < b.num_records; ++g) {
+        const int64_t H = x.rec_haps[g];
+        const int32_t R = b.reads_per_record[g];
+        int64_t sl = 0;
+        touched.clear();
+        for (int32_t r = 0; r < R; ++r, ++i) {
+            const int32_t L = b.read_lengths[i];
+            if (L < 1) { err = "read length < 1"; return PAIRHMM_ERR_INVALID_ARGUMENT; }
+            if (b.read_offsets) {
+                const int64_t o = b.read_offsets[i];
+                if (o < 0) { err = "negative read offset"; return PAIRHMM_ERR_INVALID_ARGUMENT; }
+                x.read_bytes = std::max<int64_t>(x.read_bytes, o + L);
+                x.read_min = i == 0 ? o : std::min<int64_t>(x.read_min, o);
+            }
+            x.max_read_len = std::max(x.max_read_len, L);
+            x.read_record[i] = (int32_t)g;
+            x.read_local[i] = r;
+            x.read_start[i] = x.pack_positions;
+            x.pack_positions += round_up(L, 4);
+            sl += L;
+            const int bk = L <= lut_max ? lut[L] : bucket_of_host(L, rules);
+            x.bucket_pairs[bk] += H;
+            x.class_pairs[fp64_class(L)] += H;
+            if (multi[bk]) x.multi_tile_pairs += H;
+            if (packed[bk]) {
+                if (pending[bk] < 0) {
+                    pending[bk] = (int32_t)i;
+                    touched.push_back(bk);
+                    continue;
+                }
+                x.unit_read0.push_back(pending[bk]);
+                x.unit_read1.push_back((int32_t)i);
+                pending[bk] = -1;
+            } else {
+                x.unit_read0.push_back((int32_t)i);
+                x.unit_read1.push_back(-1);
+            }
+            x.unit_bucket.push_back(bk);
+            x.bucket_items[bk] += H;
+        }
+        for (int bk : touched)
+            if (pending[bk] >= 0) {
+                x.unit_read0.push_back(pending[bk]);
+                x.unit_read1.push_back(-1);
                 x.unit_bucket.push_back(bk);
                 x.bucket_items[bk] += H;
+                pending[bk] = -1;
             }
-            for (int bk : touched)
-                if (pending[bk] >= 0) {
-                    x.unit_read0.push_back(pending[bk]);
-                    x.unit_read1.push_back(-1);
-                    x.unit_bucket.push_back(bk);
-                    x.bucket_items[bk] += H;
-                    pending[bk] = -1;
-                }
-        }
+        x.cells += sl * rec_hap_sum[g];
     }
-    // cells: sum over records of (sum L) * (sum H)  (gpuworker.cuh:495-520)
-    {
-        int64_t i = 0;
-        for (int64_t g = 0; g < b.num_records; ++g) {
-            int64_t sl = 0, sh = 0;
-            for (int32_t r = 0; r < b.reads_per_record[g]; ++r, ++i) sl += b.read_lengths[i];
-            for (int32_t h = 0; h < b.haps_per_record[g]; ++h) sh += b.hap_lengths[x.rec_hap_base[g] + h];
-            x.cells += sl * sh;
-        }
+    return PAIRHMM_OK;
+}
+
+pairhmm_status_t Engine::scan_inputs(const pairhmm_batch_t& b, InputRanges& r, std::string& err) {
+    r = InputRanges{};
+    if (b.num_records < 0) { err = "num_records < 0"; return PAIRHMM_ERR_INVALID_ARGUMENT; }
+    if (b.num_records == 0) return PAIRHMM_OK;
+    if (!b.reads_per_record || !b.haps_per_record) { err = "null record arrays"; return PAIRHMM_ERR_INVALID_ARGUMENT; }
+    for (int64_t g = 0; g < b.num_records; ++g) {
+        const int32_t R = b.reads_per_record[g], H = b.haps_per_record[g];
+        if (R < 0 || H < 0) { err = "negative reads/haplotypes in a record"; return PAIRHMM_ERR_INVALID_ARGUMENT; }
+        r.num_reads += R;
+        r.num_haps += H;
+        r.num_pairs += (int64_t)R * H;
     }
+    if (r.num_reads >= (int64_t(1) << 31) || r.num_haps >= (int64_t(1) << 31)) {
+        err = "more than 2^31-1 reads or haplotypes in one batch";
+        return PAIRHMM_ERR_INVALID_ARGUMENT;
+    }
+    if (r.num_reads > 0 && (!b.read_lengths || !b.read_offsets || !b.read_bases || !b.base_quals || !b.ins_quals ||
+                            !b.del_quals)) {
+        err = "null read arrays";
+        return PAIRHMM_ERR_INVALID_ARGUMENT;
+    }
+    if (r.num_haps > 0 && (!b.hap_lengths || !b.hap_offsets || !b.hap_bases)) {
+        err = "null haplotype arrays";
+        return PAIRHMM_ERR_INVALID_ARGUMENT;
+    }
+    for (int64_t i = 0; i < r.num_reads; ++i) {
+        const int32_t L = b.read_lengths[i];
+        const int64_t o = b.read_offsets[i];
+        if (L < 1) { err = "read length < 1"; return PAIRHMM_ERR_INVALID_ARGUMENT; }
+        if (o < 0) { err = "negative read offset"; return PAIRHMM_ERR_INVALID_ARGUMENT; }
+        r.read_min = i == 0 ? o : std::min(r.read_min, o);
+        r.read_end = std::max(r.read_end, o + L);
+    }
+    for (int64_t h = 0; h < r.num_haps; ++h) {
+        const int32_t H = b.hap_lengths[h];
+        const int64_t o = b.hap_offsets[h];
+        if (H < 1) { err = "haplotype length < 1"; return PAIRHMM_ERR_INVALID_ARGUMENT; }
+        if (o < 0) { err = "negative haplotype offset"; return PAIRHMM_ERR_INVALID_ARGUMENT; }
+        r.hap_min = h == 0 ? o : std::min(r.hap_min, o);
+        r.hap_end = std::max(r.hap_end, o + H);
+    }
+    return PAIRHMM_OK;
+}
+
+pairhmm_status_t Engine::ensure_inputs(const InputRanges& r) {
+    const int64_t nr = std::max<int64_t>(r.num_reads, 1), nh = std::max<int64_t>(r.num_haps, 1);
+    const int64_t rb = std::max<int64_t>(r.read_end - r.read_min, 1);
+    const int64_t hb = std::max<int64_t>(r.hap_end - r.hap_min, 1);
+    PHMM_CUDA(in_read_bases_.ensure(rb));
+    PHMM_CUDA(in_bq_.ensure(rb));
+    PHMM_CUDA(in_iq_.ensure(rb));
+    PHMM_CUDA(in_dq_.ensure(rb));
+    PHMM_CUDA(in_read_off_.ensure(8 * nr));
+    PHMM_CUDA(in_read_len_.ensure(4 * nr));
+    PHMM_CUDA(in_hap_bases_.ensure(hb));
+    PHMM_CUDA(in_hap_off_.ensure(8 * nh));
+    PHMM_CUDA(in_hap_len_.ensure(4 * nh));
+    PHMM_CUDA(scores_.ensure(4 * std::max<int64_t>(r.num_pairs, 1)));
     return PAIRHMM_OK;
 }
 
@@ -357,40 +444,19 @@ pairhmm_status_t Engine::ensure_buffers(const BatchIndex& x, bool host_inputs) {
 }
 
 pairhmm_status_t Engine::upload_index(const BatchIndex& x, cudaStream_t s) {
-    struct Piece { DevBuf* dst; const void* src; size_t bytes; };
-    const Piece pieces[] = {
-        {&read_record_, x.read_record.data(), 4 * x.read_record.size()},
-        {&read_local_, x.read_local.data(), 4 * x.read_local.size()},
-        {&rec_haps_, x.rec_haps.data(), 4 * x.rec_haps.size()},
-        {&rec_hap_base_, x.rec_hap_base.data(), 8 * x.rec_hap_base.size()},
-        {&rec_pair_base_, x.rec_pair_base.data(), 8 * x.rec_pair_base.size()},
-        {&read_start_, x.read_start.data(), 8 * x.read_start.size()},
-        {&hap_start_, x.hap_start.data(), 8 * x.hap_start.size()},
-        {&unit_read0_, x.unit_read0.data(), 4 * x.unit_read0.size()},
-        {&unit_read1_, x.unit_read1.data(), 4 * x.unit_read1.size()},
-        {&unit_bucket_, x.unit_bucket.data(), 4 * x.unit_bucket.size()},
+    const std::vector<HostUploader::Copy> copies = {
+        {read_record_.ptr, x.read_record.data(), 4 * x.read_record.size()},
+        {read_local_.ptr, x.read_local.data(), 4 * x.read_local.size()},
+        {rec_haps_.ptr, x.rec_haps.data(), 4 * x.rec_haps.size()},
+        {rec_hap_base_.ptr, x.rec_hap_base.data(), 8 * x.rec_hap_base.size()},
+        {rec_pair_base_.ptr, x.rec_pair_base.data(), 8 * x.rec_pair_base.size()},
+        {read_start_.ptr, x.read_start.data(), 8 * x.read_start.size()},
+        {hap_start_.ptr, x.hap_start.data(), 8 * x.hap_start.size()},
+        {unit_read0_.ptr, x.unit_read0.data(), 4 * x.unit_read0.size()},
+        {unit_read1_.ptr, x.unit_read1.data(), 4 * x.unit_read1.size()},
+        {unit_bucket_.ptr, x.unit_bucket.data(), 4 * x.unit_bucket.size()},
     };
-    size_t total = 0;
-    for (const Piece& p : pieces) total += round_up((int64_t)p.bytes, 256);
-    if (total > pinned_cap_) {
-        PHMM_CUDA(cudaStreamSynchronize(s));
-        if (pinned_) cudaFreeHost(pinned_);
-        pinned_ = nullptr;
-        pinned_cap_ = 0;
-        PHMM_CUDA(cudaMallocHost(&pinned_, total + total / 4));
-        pinned_cap_ = total + total / 4;
-    } else {
-        // the previous upload may still be in flight
-        PHMM_CUDA(cudaStreamSynchronize(s));
-    }
-    size_t off = 0;
-    for (const Piece& p : pieces) {
-        if (p.bytes == 0) continue;
-        char* dst = static_cast<char*>(pinned_) + off;
-        std::memcpy(dst, p.src, p.bytes);
-        PHMM_CUDA(cudaMemcpyAsync(p.dst->ptr, dst, p.bytes, cudaMemcpyHostToDevice, s));
-        off += round_up((int64_t)p.bytes, 256);
-    }
+    PHMM_CUDA(uploader_.run(opts_.device, copies, s));
     return PAIRHMM_OK;
 }
 
@@ -618,34 +684,43 @@ pairhmm_status_t Engine::run_pipeline(const pairhmm_batch_t& in, const BatchInde
 pairhmm_status_t Engine::compute_host(const pairhmm_batch_t& b, float* scores) {
     const auto t0 = std::chrono::steady_clock::now();
     PHMM_CUDA(cudaSetDevice(opts_.device));
-    BatchIndex x;
+    // first a cheap validating pass for sizes and byte ranges, so the input
+    // upload runs on helper threads while this thread builds the index
+    InputRanges rg;
     std::string err;
-    pairhmm_status_t st = build_index(b, rules_, x, err);
+    pairhmm_status_t st = scan_inputs(b, rg, err);
     if (st != PAIRHMM_OK) return fail(st, err);
-    if (x.num_pairs > 0 && !scores) return fail(PAIRHMM_ERR_INVALID_ARGUMENT, "null scores");
-    if (x.num_reads > 0 && (!b.read_bases || !b.base_quals || !b.ins_quals || !b.del_quals || !b.read_offsets))
-        return fail(PAIRHMM_ERR_INVALID_ARGUMENT, "null read arrays");
-    if (x.num_haps > 0 && (!b.hap_bases || !b.hap_offsets)) return fail(PAIRHMM_ERR_INVALID_ARGUMENT, "null haplotype arrays");
+    if (rg.num_pairs > 0 && !scores) return fail(PAIRHMM_ERR_INVALID_ARGUMENT, "null scores");
     stats_ = pairhmm_stats_t{};
-    stats_.pairs = x.num_pairs;
-    stats_.cells = x.cells;
-    stats_.multi_tile_pairs = x.multi_tile_pairs;
-    if (x.num_pairs == 0) return PAIRHMM_OK;
-    if ((st = ensure_buffers(x, true)) != PAIRHMM_OK) return st;
+    if (rg.num_pairs == 0) return PAIRHMM_OK;
+    if ((st = ensure_inputs(rg)) != PAIRHMM_OK) return st;
     cudaStream_t s = stream_;
     // only the byte range the batch references is copied; device base pointers
     // are shifted so the caller's absolute offsets stay valid
-    const int64_t rlo = x.read_min, rn = x.read_bytes - x.read_min;
-    const int64_t hlo = x.hap_min, hn = x.hap_bytes - x.hap_min;
-    PHMM_CUDA(cudaMemcpyAsync(in_read_bases_.ptr, b.read_bases + rlo, rn, cudaMemcpyHostToDevice, s));
-    PHMM_CUDA(cudaMemcpyAsync(in_bq_.ptr, b.base_quals + rlo, rn, cudaMemcpyHostToDevice, s));
-    PHMM_CUDA(cudaMemcpyAsync(in_iq_.ptr, b.ins_quals + rlo, rn, cudaMemcpyHostToDevice, s));
-    PHMM_CUDA(cudaMemcpyAsync(in_dq_.ptr, b.del_quals + rlo, rn, cudaMemcpyHostToDevice, s));
-    PHMM_CUDA(cudaMemcpyAsync(in_read_off_.ptr, b.read_offsets, 8 * x.num_reads, cudaMemcpyHostToDevice, s));
-    PHMM_CUDA(cudaMemcpyAsync(in_read_len_.ptr, b.read_lengths, 4 * x.num_reads, cudaMemcpyHostToDevice, s));
-    PHMM_CUDA(cudaMemcpyAsync(in_hap_bases_.ptr, b.hap_bases + hlo, hn, cudaMemcpyHostToDevice, s));
-    PHMM_CUDA(cudaMemcpyAsync(in_hap_off_.ptr, b.hap_offsets, 8 * x.num_haps, cudaMemcpyHostToDevice, s));
-    PHMM_CUDA(cudaMemcpyAsync(in_hap_len_.ptr, b.hap_lengths, 4 * x.num_haps, cudaMemcpyHostToDevice, s));
+    const int64_t rlo = rg.read_min, rn = rg.read_end - rg.read_min;
+    const int64_t hlo = rg.hap_min, hn = rg.hap_end - rg.hap_min;
+    const std::vector<HostUploader::Copy> inputs = {
+        {in_read_bases_.ptr, b.read_bases + rlo, (size_t)rn},
+        {in_bq_.ptr, b.base_quals + rlo, (size_t)rn},
+        {in_iq_.ptr, b.ins_quals + rlo, (size_t)rn},
+        {in_dq_.ptr, b.del_quals + rlo, (size_t)rn},
+        {in_read_off_.ptr, b.read_offsets, (size_t)(8 * rg.num_reads)},
+        {in_read_len_.ptr, b.read_lengths, (size_t)(4 * rg.num_reads)},
+        {in_hap_bases_.ptr, b.hap_bases + hlo, (size_t)hn},
+        {in_hap_off_.ptr, b.hap_offsets, (size_t)(8 * rg.num_haps)},
+        {in_hap_len_.ptr, b.hap_lengths, (size_t)(4 * rg.num_haps)},
+    };
+    cudaError_t up = cudaSuccess;
+    std::thread uploader([&] { up = uploader_.run(opts_.device, inputs, s); });
+    st = build_index(b, rules_, idx_, err);
+    uploader.join();
+    if (up != cudaSuccess) return cuda_fail(up, "input upload");
+    if (st != PAIRHMM_OK) return fail(st, err);
+    const BatchIndex& x = idx_;
+    stats_.pairs = x.num_pairs;
+    stats_.cells = x.cells;
+    stats_.multi_tile_pairs = x.multi_tile_pairs;
+    if ((st = ensure_buffers(x, false)) != PAIRHMM_OK) return st;
     if ((st = upload_index(x, s)) != PAIRHMM_OK) return st;
 
     pairhmm_batch_t dev = b;
@@ -713,9 +788,9 @@ pairhmm_status_t Engine::compute_device(const pairhmm_batch_t& b, int32_t, int32
     hb.hap_lengths = hl.data();
     hb.read_offsets = nullptr;
     hb.hap_offsets = nullptr;
-    BatchIndex x;
     std::string err;
-    pairhmm_status_t st = build_index(hb, rules_, x, err);
+    pairhmm_status_t st = build_index(hb, rules_, idx_, err);
+    const BatchIndex& x = idx_;
     if (st != PAIRHMM_OK) return fail(st, err);
     stats_ = pairhmm_stats_t{};
     stats_.pairs = x.num_pairs;

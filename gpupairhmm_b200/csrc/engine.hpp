@@ -8,6 +8,7 @@
 #include <vector>
 
 #include "../../include/pairhmm_b200.h"
+#include "host_upload.hpp"
 #include "kernels.hpp"
 
 namespace phmm {
@@ -36,6 +37,13 @@ struct BatchIndex {
     std::vector<int32_t> unit_read0, unit_read1, unit_bucket;  // units: 1 or 2 reads of a record
     int64_t class_pairs[kFp64Classes] = {};         // by FP64 length class (fp64_class)
     int64_t multi_tile_pairs = 0;
+};
+
+// Sizes and referenced byte ranges of a host batch, validated (first pass,
+// cheap: lets the input upload start before the index is built).
+struct InputRanges {
+    int64_t num_reads = 0, num_haps = 0, num_pairs = 0;
+    int64_t read_min = 0, read_end = 0, hap_min = 0, hap_end = 0;
 };
 
 // Grow-only device buffer.
@@ -72,6 +80,7 @@ public:
 
     static pairhmm_status_t build_index(const pairhmm_batch_t& b, const std::vector<TileRule>& rules,
                                         BatchIndex& idx, std::string& err);
+    static pairhmm_status_t scan_inputs(const pairhmm_batch_t& b, InputRanges& r, std::string& err);
 
 private:
     pairhmm_status_t upload_rules();
@@ -89,6 +98,7 @@ private:
     pairhmm_status_t enqueue_pipeline(const pairhmm_batch_t& dev_in, const BatchIndex& idx, const Plan& plan,
                                       float* d_scores, cudaStream_t s, int stage);
     pairhmm_status_t ensure_buffers(const BatchIndex& idx, bool host_inputs);
+    pairhmm_status_t ensure_inputs(const InputRanges& r);
     pairhmm_status_t upload_index(const BatchIndex& idx, cudaStream_t s);
     int persistent_grid(const void* kernel, size_t smem) const;
     static int64_t index_bytes(const BatchIndex& x);
@@ -113,9 +123,9 @@ private:
     DevBuf unit_read0_, unit_read1_, unit_bucket_;
     DevBuf read_pack_, hap_code_, hist_, cursor_, items_, rescue_, counters_, sched_, scores_, scratch_;
     DevBuf lens_tmp_;
-    // pinned staging for the index upload
-    void* pinned_ = nullptr;
-    size_t pinned_cap_ = 0;
+    // host-to-device uploads (caller inputs, index) and the reused index
+    HostUploader uploader_;
+    BatchIndex idx_;
 };
 
 }  // namespace phmm

@@ -1,0 +1,85 @@
+#include "host_upload.hpp"
+
+#include <algorithm>
+#include <cstring>
+#include <thread>
+
+namespace phmm {
+
+HostUploader::~HostUploader() {
+    for (cudaEvent_t& e : done_)
+        if (e) cudaEventDestroy(e);
+    if (stage_) cudaFreeHost(stage_);
+}
+
+bool HostUploader::is_page_locked(const void* p) {
+    cudaPointerAttributes a{};
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();  // pageable memory on older runtimes reports an error; clear it
+        return false;
+    }
+    return a.type == cudaMemoryTypeHost;
+}
+
+cudaError_t HostUploader::ensure_staging() {
+    if (stage_) return cudaSuccess;
+    void* p = nullptr;
+    cudaError_t e = cudaMallocHost(&p, kSlotBytes * kThreads * kSlotsPerThread);
+    if (e != cudaSuccess) return e;
+    stage_ = static_cast<char*>(p);
+    for (cudaEvent_t& ev : done_)
+        if ((e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming)) != cudaSuccess) return e;
+    return cudaSuccess;
+}
+
+cudaError_t HostUploader::run(int device, const std::vector<Copy>& copies, cudaStream_t s) {
+    staged_ = direct_ = 0;
+    cudaError_t e = cudaSetDevice(device);
+    if (e != cudaSuccess) return e;
+    struct Piece {
+        char* dst;
+        const char* src;
+        size_t bytes;
+    };
+    std::vector<Piece> pieces;
+    for (const Copy& c : copies) {
+        if (c.bytes == 0) continue;
+        if (is_page_locked(c.src)) {
+            if ((e = cudaMemcpyAsync(c.dst, c.src, c.bytes, cudaMemcpyHostToDevice, s)) != cudaSuccess) return e;
+            direct_ += c.bytes;
+            continue;
+        }
+        for (size_t off = 0; off < c.bytes; off += kSlotBytes)
+            pieces.push_back({static_cast<char*>(c.dst) + off, static_cast<const char*>(c.src) + off,
+                              std::min(kSlotBytes, c.bytes - off)});
+        staged_ += c.bytes;
+    }
+    if (pieces.empty()) return cudaSuccess;
+    if ((e = ensure_staging()) != cudaSuccess) return e;
+    const int nthreads = (int)std::min<size_t>(kThreads, pieces.size());
+    cudaError_t err[kThreads] = {};
+    auto worker = [&](int t) {
+        cudaError_t r = cudaSetDevice(device);
+        int j = 0;
+        for (size_t k = (size_t)t; k < pieces.size() && r == cudaSuccess; k += (size_t)nthreads, ++j) {
+            const int slot = t * kSlotsPerThread + (j % kSlotsPerThread);
+            char* buf = stage_ + (size_t)slot * kSlotBytes;
+            // the slot's previous DMA (this run or an earlier one) must be done
+            if ((r = cudaEventSynchronize(done_[slot])) != cudaSuccess) break;
+            std::memcpy(buf, pieces[k].src, pieces[k].bytes);
+            if ((r = cudaMemcpyAsync(pieces[k].dst, buf, pieces[k].bytes, cudaMemcpyHostToDevice, s)) != cudaSuccess)
+                break;
+            r = cudaEventRecord(done_[slot], s);
+        }
+        err[t] = r;
+    };
+    std::vector<std::thread> threads;
+    for (int t = 1; t < nthreads; ++t) threads.emplace_back(worker, t);
+    worker(0);
+    for (std::thread& th : threads) th.join();
+    for (int t = 0; t < nthreads; ++t)
+        if (err[t] != cudaSuccess) return err[t];
+    return cudaSuccess;
+}
+
+}  // namespace phmm
