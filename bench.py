@@ -60,6 +60,9 @@ def parse_args():
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU baseline sample size (seconds of work)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--accuracy-pairs", type=int, default=3000)
+    ap.add_argument("--serving-seconds", type=float, default=10.0,
+                    help="length of the streaming-service run (0 = skip); the full configuration is 60")
+    ap.add_argument("--serving-rate", type=float, default=2000.0, help="region arrivals per second")
     return ap.parse_args()
 
 
@@ -237,6 +240,70 @@ def run_binary(args, cfg):
                                 "parsing excluded), whole batch at once"}), flush=True)
 
 
+def percentile(xs, q):
+    return float(np.percentile(np.asarray(xs, dtype=np.float64), q)) if len(xs) else None
+
+
+def run_serving(args, local_rank):
+    """Streaming service: regions arrive as a Poisson stream (the uneven-length
+    region shapes, 5% long-read shapes) and are submitted to the engine's
+    continuous-batching queue as they arrive; each region's latency is from
+    submission to results ready on the host.  Beside it, the same stream through
+    one blocking plain-FP32 call per region in arrival order (latency from
+    arrival, so it includes waiting behind earlier regions)."""
+    import gpupairhmm_b200 as g
+    from gpupairhmm_b200 import synth
+    stream = [(t, r.contiguous()) for t, r in synth.stream_regions(seed=4, rate=args.serving_rate,
+                                                                    seconds=args.serving_seconds)]
+    cells = sum(r.cells() for _, r in stream)
+    pairs = sum(r.num_pairs for _, r in stream)
+    out = {"regions": len(stream), "rate_per_s": args.serving_rate, "seconds": args.serving_seconds,
+           "pairs": pairs, "cells": cells, "long_region_fraction": 0.05}
+
+    # continuous batching
+    eng = g.Engine(device=local_rank)
+    warm = [eng.submit(r) for _, r in stream[:200]]  # warm the queue's engines (a burst of both kinds)
+    for tk, (_, r) in zip(warm, stream[:200]):
+        eng.drain(tk, r.num_pairs)
+    t0 = time.perf_counter()
+    tickets = []
+    for t_arr, r in stream:
+        while time.perf_counter() - t0 < t_arr:
+            pass
+        tickets.append((eng.submit(r), time.perf_counter() - t0, r.num_pairs))
+    lat, done = [], []
+    for tk, t_sub, n in tickets:
+        while not eng.poll(tk):
+            time.sleep(0.0002)
+        ms = eng.latency_ms(tk)
+        eng.drain(tk, n)
+        lat.append(ms)
+        done.append(t_sub + ms / 1e3)
+    span = max(done)
+    eng.close()
+    out["continuous_batching"] = {"p50_ms": round(percentile(lat, 50), 3), "p99_ms": round(percentile(lat, 99), 3),
+                                  "max_ms": round(max(lat), 3), "gcups": round(cells / span / 1e9, 3),
+                                  "span_s": round(span, 3)}
+
+    # one region per blocking call, plain FP32 form
+    pe = g.Engine(device=local_rank, mode=g.MODE_PLAIN)
+    for _, r in stream[:200]:
+        pe.compute(r)
+    lat = []
+    t0 = time.perf_counter()
+    for t_arr, r in stream:
+        while time.perf_counter() - t0 < t_arr:
+            pass
+        pe.compute(r)
+        lat.append((time.perf_counter() - t0 - t_arr) * 1e3)
+    span = time.perf_counter() - t0
+    pe.close()
+    out["plain_per_region"] = {"p50_ms": round(percentile(lat, 50), 3), "p99_ms": round(percentile(lat, 99), 3),
+                               "max_ms": round(max(lat), 3), "gcups": round(cells / span / 1e9, 3),
+                               "span_s": round(span, 3)}
+    return out
+
+
 def run_ours(args, cfg, rank, world, local_rank):
     import torch
     import gpupairhmm_b200 as g
@@ -256,7 +323,7 @@ def run_ours(args, cfg, rank, world, local_rank):
     mode = g.MODE_PLAIN if args.mode == "plain" else g.MODE_ENGINE
     engine = g.Engine(device=local_rank, mode=mode)
     peak = g.probe_fp32_peak(local_rank, 100)
-    scores = np.empty(batch.num_pairs, dtype=np.float32)
+    scores = torch.empty(batch.num_pairs, dtype=torch.float32).pin_memory().numpy()  # page-locked output
     for _ in range(args.warmup):
         engine.compute(pinned, out=scores)
 
@@ -331,6 +398,8 @@ def run_ours(args, cfg, rank, world, local_rank):
             gc, desc = cpu_rate(lambda b: oracle.batch_log10(b), batch, args.cpu_seconds, rng)
             line["cpu_baseline"] = {"value": round(gc, 4), "unit": "GCUPS", "cores": os.cpu_count() or 1,
                                     "kind": "port", "sample": desc + "; FP64 oracle, OpenMP over pairs"}
+        if world == 1 and args.serving_seconds > 0:
+            line["serving"] = run_serving(args, local_rank)
         print(json.dumps(line), flush=True)
     engine.close()
     if dist:

@@ -114,6 +114,8 @@ _SIGNATURES = {
     "pairhmm_records_view": (ctypes.c_int, [_P, _P, _P]),
     "pairhmm_records_format": (ctypes.c_int, [_P, _P, _P, ctypes.c_int64, _P]),
     "pairhmm_records_free": (None, [_P]),
+    "pairhmm_host_register": (ctypes.c_int, [_P, ctypes.c_size_t]),
+    "pairhmm_host_unregister": (ctypes.c_int, [_P]),
     "pairhmm_forward_pairs_noalloc": (ctypes.c_int, [ctypes.c_int32] + [_P] * 6 + [ctypes.c_int64, ctypes.c_int32,
                                                                                   _P, _P]),
 }

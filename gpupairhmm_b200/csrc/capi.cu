@@ -222,6 +222,30 @@ pairhmm_status_t pairhmm_records_format(const pairhmm_records_t* r, const float*
 
 void pairhmm_records_free(pairhmm_records_t* r) { delete r; }
 
+pairhmm_status_t pairhmm_host_register(void* ptr, size_t bytes) {
+    if (!ptr || bytes == 0) return PAIRHMM_ERR_INVALID_ARGUMENT;
+    const cudaError_t e = cudaHostRegister(ptr, bytes, cudaHostRegisterPortable);
+    if (e == cudaErrorHostMemoryAlreadyRegistered) {
+        cudaGetLastError();
+        return PAIRHMM_OK;
+    }
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return e == cudaErrorMemoryAllocation ? PAIRHMM_ERR_OUT_OF_MEMORY : PAIRHMM_ERR_CUDA;
+    }
+    return PAIRHMM_OK;
+}
+
+pairhmm_status_t pairhmm_host_unregister(void* ptr) {
+    if (!ptr) return PAIRHMM_ERR_INVALID_ARGUMENT;
+    const cudaError_t e = cudaHostUnregister(ptr);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return PAIRHMM_ERR_INVALID_ARGUMENT;
+    }
+    return PAIRHMM_OK;
+}
+
 const char* pairhmm_version(void) { return "pairhmm_b200 0.1.0 (sm_100a)"; }
 
 pairhmm_status_t pairhmm_set_tile_table(pairhmm_engine_t* h, const int32_t* max_len, const int32_t* group,

@@ -45,6 +45,29 @@ struct Options {
 struct PipelineData {
     phmm::HostBatch batch;
     std::vector<float> scores;
+    std::vector<void*> pinned;  // batch arrays page-locked by the parser thread
+
+    // page-lock the parsed arrays so the engine uploads them by DMA; a failed
+    // registration only means that array is staged through the engine's buffers
+    void pin() {
+        auto reg = [&](void* p, size_t n) {
+            if (n && pairhmm_host_register(p, n) == PAIRHMM_OK) pinned.push_back(p);
+        };
+        phmm::HostBatch& b = batch;
+        reg(b.read_bases.data(), b.read_bases.size());
+        reg(b.base_quals.data(), b.base_quals.size());
+        reg(b.ins_quals.data(), b.ins_quals.size());
+        reg(b.del_quals.data(), b.del_quals.size());
+        reg(b.hap_bases.data(), b.hap_bases.size());
+        reg(b.read_offsets.data(), 8 * b.read_offsets.size());
+        reg(b.read_lengths.data(), 4 * b.read_lengths.size());
+        reg(b.hap_offsets.data(), 8 * b.hap_offsets.size());
+        reg(b.hap_lengths.data(), 4 * b.hap_lengths.size());
+    }
+    void unpin() {
+        for (void* p : pinned) pairhmm_host_unregister(p);
+        pinned.clear();
+    }
 };
 
 template <class T>
@@ -81,9 +104,11 @@ void parser_thread(const Options& o, Queue<PipelineData*>* in, Queue<PipelineDat
     if (!reader.ok()) die(reader.error());
     for (;;) {
         PipelineData* d = in->pop();
+        d->unpin();
         d->batch.clear();
         bool eof = false;
         if (!reader.next(d->batch, o.fileBatchsize, eof)) die("parse error: " + reader.error());
+        d->pin();
         if (d->batch.num_records() > 0) out->push(d);
         else in->push(d);
         if (eof) break;
@@ -99,6 +124,18 @@ void gpu_thread(const Options& o, Queue<PipelineData*>* in, Queue<PipelineData*>
     pairhmm_engine_t* eng = nullptr;
     pairhmm_status_t st = pairhmm_engine_create(&eo, &eng);
     if (st != PAIRHMM_OK) die(std::string("engine: ") + pairhmm_status_string(st));
+    {
+        // one tiny batch before the timed loop sets up what a first call would
+        // (streams, graphs, staging buffers), as the reference warms its
+        // memory pool before timing (main.cu:31-43)
+        std::string err;
+        phmm::HostBatch warm;
+        if (phmm::parse_records("1 1\nACGT IIII IIII IIII ++++\nACGTACGT\n", warm, err)) {
+            const pairhmm_batch_t v = warm.view();
+            float score = 0.f;
+            pairhmm_compute_host(eng, &v, &score);
+        }
+    }
     for (;;) {
         PipelineData* d = in->pop();
         if (!d) break;
@@ -172,6 +209,9 @@ void writer_thread(const Options& o, Queue<PipelineData*>* in, Queue<PipelineDat
 }  // namespace
 
 int main(int argc, char** argv) {
+    // load every kernel when the device is set up, not at its first launch
+    // inside the timed batches
+    setenv("CUDA_MODULE_LOADING", "EAGER", 0);
     Options o;
     for (int x = 1; x < argc; ++x) {
         const std::string a = argv[x];
@@ -216,6 +256,7 @@ int main(int argc, char** argv) {
     tp.join();
     tg.join();
     tw.join();
+    for (auto& b : buffers) b->unpin();
     const double gcups = seconds > 0 ? cells / 1e9 / seconds : 0.0;
     std::cout << "Batch processing time: " << seconds << "s (" << gcups << " GCUPS)\n";
     return 0;

@@ -92,6 +92,7 @@ Engine::~Engine() {
                       &hap_start_, &read_pack_, &hap_code_, &hist_, &cursor_, &items_, &rescue_, &counters_,
                       &sched_, &scores_, &scratch_, &lens_tmp_, &unit_read0_, &unit_read1_, &unit_bucket_};
     for (DevBuf* b : bufs) b->release();
+    if (host_out_) cudaFreeHost(host_out_);
     if (ev0_) cudaEventDestroy(ev0_);
     if (ev1_) cudaEventDestroy(ev1_);
     if (ev_prep_) cudaEventDestroy(ev_prep_);
@@ -503,9 +504,19 @@ pairhmm_status_t Engine::enqueue_pipeline(const pairhmm_batch_t& in, const Batch
     pa.hap_code = hap_code_.as<uint8_t>();
     if (stage == 0) {
     launches_ = 0;
+    // zero the histogram and the work/rescue counters, pad the haplotype codes
+    // (a kernel, not memset nodes: see launch_fill)
+    {
+        uint8_t* const ptr[3] = {hap_code_.as<uint8_t>() + x.code_bytes, hist_.as<uint8_t>(),
+                                 counters_.as<uint8_t>()};
+        const long long bytes[3] = {kHapSlack, (long long)sizeof(unsigned int) * nb * (plain ? 1 : kHBins),
+                                    (long long)sizeof(unsigned long long) * (kMaxBuckets + 2 * kFp64Classes)};
+        const int value[3] = {4, 0, 0};
+        PHMM_CUDA(launch_fill(ptr, bytes, value, 3, s));
+        launches_ += 1;
+    }
     PHMM_CUDA(launch_pack(pa, prep_grid, s));
     launches_ += 2;
-    PHMM_CUDA(cudaMemsetAsync(hap_code_.as<uint8_t>() + x.code_bytes, 4, kHapSlack, s));
     }
 
     BinArgs ba{};
@@ -528,7 +539,6 @@ pairhmm_status_t Engine::enqueue_pipeline(const pairhmm_batch_t& in, const Batch
     if (stage == 0) {
     PHMM_CUDA(launch_binning(ba, prep_grid, s, per_task_.as<int>(), config_.as<int>(), sched_.as<Schedule>(), nb));
     launches_ += 4;
-    PHMM_CUDA(cudaMemsetAsync(counters_.ptr, 0, sizeof(unsigned long long) * (kMaxBuckets + 2 * kFp64Classes), s));
     return PAIRHMM_OK;
     }
 
@@ -740,11 +750,27 @@ pairhmm_status_t Engine::compute_host(const pairhmm_batch_t& b, float* scores) {
 
     PHMM_CUDA(cudaEventRecord(ev0_, s));
     if ((st = run_pipeline(dev, x, scores_.as<float>(), s)) != PAIRHMM_OK) return st;
-    PHMM_CUDA(cudaMemcpyAsync(scores, scores_.ptr, 4 * x.num_pairs, cudaMemcpyDeviceToHost, s));
+    // scores go straight into a page-locked caller buffer; otherwise through
+    // this engine's page-locked staging (a copy into pageable memory would
+    // hold the driver's pageable-copy path while it waits for this stream)
+    const bool direct = HostUploader::is_page_locked(scores);
+    const size_t stage_bytes = 64 + (direct ? 0 : 4 * (size_t)x.num_pairs);
+    if (stage_bytes > host_out_cap_) {
+        if (host_out_) cudaFreeHost(host_out_);
+        host_out_ = nullptr;
+        host_out_cap_ = 0;
+        PHMM_CUDA(cudaMallocHost(&host_out_, stage_bytes + stage_bytes / 4));
+        host_out_cap_ = stage_bytes + stage_bytes / 4;
+    }
+    float* dst = direct ? scores : reinterpret_cast<float*>(static_cast<char*>(host_out_) + 64);
+    PHMM_CUDA(cudaMemcpyAsync(dst, scores_.ptr, 4 * x.num_pairs, cudaMemcpyDeviceToHost, s));
     unsigned long long rescued_by_class[kFp64Classes] = {};
-    PHMM_CUDA(cudaMemcpyAsync(rescued_by_class, counters_.as<unsigned long long>() + kMaxBuckets,
+    static_assert(sizeof(rescued_by_class) <= 64, "rescue counts fit the staging header");
+    PHMM_CUDA(cudaMemcpyAsync(host_out_, counters_.as<unsigned long long>() + kMaxBuckets,
                               sizeof(rescued_by_class), cudaMemcpyDeviceToHost, s));
     PHMM_CUDA(cudaStreamSynchronize(s));
+    if (!direct) std::memcpy(scores, dst, 4 * (size_t)x.num_pairs);
+    std::memcpy(rescued_by_class, host_out_, sizeof(rescued_by_class));
     float ms = 0.f, a = 0.f, b2 = 0.f, c = 0.f;
     PHMM_CUDA(cudaEventElapsedTime(&ms, ev0_, ev1_));
     PHMM_CUDA(cudaEventElapsedTime(&a, ev0_, ev_prep_));

@@ -126,6 +126,9 @@ private:
     // host-to-device uploads (caller inputs, index) and the reused index
     HostUploader uploader_;
     BatchIndex idx_;
+    // page-locked staging for the download: rescue counts, then scores
+    void* host_out_ = nullptr;
+    size_t host_out_cap_ = 0;
 };
 
 }  // namespace phmm

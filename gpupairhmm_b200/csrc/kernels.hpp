@@ -67,6 +67,8 @@ int fp64_per_warp(int cls);
 
 // Preparation kernels.
 cudaError_t launch_pack(const PrepArgs& a, int grid, cudaStream_t s);
+// byte fills of n <= kFillRanges device ranges in one kernel launch
+cudaError_t launch_fill(uint8_t* const* ptr, const long long* bytes, const int* value, int n, cudaStream_t s);
 cudaError_t launch_binning(BinArgs a, int grid, cudaStream_t s, const int* per_task_dev,
                            const int* config_dev, Schedule* sched, int nranks);
 

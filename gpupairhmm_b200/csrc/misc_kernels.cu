@@ -107,13 +107,26 @@ cudaError_t launch_pack(const PrepArgs& a, int grid, cudaStream_t s) {
     return cudaGetLastError();
 }
 
+cudaError_t launch_fill(uint8_t* const* ptr, const long long* bytes, const int* value, int n, cudaStream_t s) {
+    FillArgs a{};
+    long long most = 0;
+    for (int k = 0; k < kFillRanges; ++k) {
+        a.ptr[k] = k < n ? ptr[k] : nullptr;
+        a.bytes[k] = k < n ? bytes[k] : 0;
+        a.value[k] = k < n ? value[k] : 0;
+        most = a.bytes[k] > most ? a.bytes[k] : most;
+    }
+    if (most == 0) return cudaSuccess;
+    const long long blocks = (most + 255) / 256;
+    fill_kernel<<<(int)(blocks < 1024 ? blocks : 1024), 256, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_binning(BinArgs a, int grid, cudaStream_t s, const int* per_task_dev,
                            const int* config_dev, Schedule* sched, int nranks) {
     const int nbins = a.nbuckets * a.hbins;
-    cudaError_t e = cudaMemsetAsync(a.hist, 0, sizeof(unsigned int) * nbins, s);
-    if (e != cudaSuccess) return e;
     bin_count_kernel<<<grid, 256, 0, s>>>(a);
-    hist_scan_kernel<<<1, 1024, 0, s>>>(a.hist, a.cursor, nbins);
+    hist_scan_kernel<<<1, kHistScanThreads, 0, s>>>(a.hist, a.cursor, nbins);
     schedule_kernel<<<1, 32, 0, s>>>(a.cursor, a.hist, nranks, a.hbins, per_task_dev, config_dev, sched);
     bin_scatter_kernel<<<grid, 256, 0, s>>>(a);
     return cudaGetLastError();

@@ -159,9 +159,29 @@ __global__ void bin_scatter_kernel(BinArgs a) {
     }
 }
 
-// single-block exclusive scan of the histogram into cursor (n up to a few 1e5)
-__global__ void hist_scan_kernel(const unsigned int* hist, unsigned long long* cursor, int n) {
-    __shared__ unsigned long long part[1024];
+// Byte fills of up to kFillRanges device ranges in one launch.  Used instead of
+// cudaMemsetAsync inside the captured stages: a memset node may be run by a
+// copy engine, where it queues behind other streams' pending copies.
+constexpr int kFillRanges = 3;
+struct FillArgs {
+    uint8_t* ptr[kFillRanges];
+    long long bytes[kFillRanges];
+    int value[kFillRanges];
+};
+__global__ void fill_kernel(FillArgs a) {
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (int k = 0; k < kFillRanges; ++k)
+        for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < a.bytes[k]; i += stride)
+            a.ptr[k][i] = (uint8_t)a.value[k];
+}
+
+// single-block exclusive scan of the histogram into cursor (n up to a few 1e5).
+// The block is kept small (kHistScanThreads) so that it finds room on an SM
+// next to the long-running blocks of another engine's kernels.
+constexpr int kHistScanThreads = 256;
+__global__ void __launch_bounds__(kHistScanThreads)
+hist_scan_kernel(const unsigned int* hist, unsigned long long* cursor, int n) {
+    __shared__ unsigned long long part[kHistScanThreads];
     const int tid = threadIdx.x;
     const int per = (n + blockDim.x - 1) / blockDim.x;
     const int b = tid * per;

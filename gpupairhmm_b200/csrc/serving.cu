@@ -14,6 +14,8 @@ ServingQueue::ServingQueue(Engine& parent) : parent_(parent) {
     // the parent's options carry the budget; each slot gets an equal share
     const int64_t budget = parent.budget_bytes() > 0 ? parent.budget_bytes() : kDefaultBudget;
     budget_per_slot_ = budget / kSlots;
+    for (const TileRule& r : parent.tile_table())
+        if (!r.multi_tile) single_tile_max_ = std::max(single_tile_max_, r.max_len);
 }
 
 ServingQueue::~ServingQueue() {
@@ -79,6 +81,7 @@ pairhmm_status_t ServingQueue::submit(const pairhmm_batch_t& b, uint64_t* ticket
     for (int64_t h = 0; h < x.num_haps; ++h)
         std::memcpy(&r->hap_bases[r->hap_off[h]], b.hap_bases + b.hap_offsets[h], b.hap_lengths[h]);
     r->pairs = x.num_pairs;
+    r->heavy = x.max_read_len > single_tile_max_;
     r->device_bytes = estimate_device_bytes(*r);
     if (r->device_bytes > budget_per_slot_) {
         error_ = "region needs more device memory than one batch slot's budget";
@@ -108,36 +111,37 @@ pairhmm_status_t ServingQueue::submit(const pairhmm_batch_t& b, uint64_t* ticket
         }
         r->ticket = next_ticket_++;
         tickets_[r->ticket] = r;
-        queue_.push_back(r);
+        (r->heavy ? heavy_ : light_).push_back(r);
         *ticket = r->ticket;
     }
-    cv_work_.notify_one();
+    cv_work_.notify_all();
     return PAIRHMM_OK;
 }
 
 void ServingQueue::worker(int slot) {
     Engine& eng = *engines_[slot];
+    std::deque<std::shared_ptr<Region>>& queue = slot < kLightSlots ? light_ : heavy_;
     for (;;) {
         std::vector<std::shared_ptr<Region>> take;
         bool more = false;
         {
             std::unique_lock<std::mutex> lk(mu_);
-            cv_work_.wait(lk, [&] { return stop_ || !queue_.empty(); });
-            if (stop_ && queue_.empty()) return;
+            cv_work_.wait(lk, [&] { return stop_ || !queue.empty(); });
+            if (stop_ && queue.empty()) return;
             // admission: everything queued that fits this slot's budget
             int64_t bytes = 0, pairs = 0;
-            while (!queue_.empty()) {
-                const auto& r = queue_.front();
+            while (!queue.empty()) {
+                const auto& r = queue.front();
                 if (!take.empty() && (bytes + r->device_bytes > budget_per_slot_ || pairs + r->pairs > kMaxBatchPairs))
                     break;
                 bytes += r->device_bytes;
                 pairs += r->pairs;
                 take.push_back(r);
-                queue_.pop_front();
+                queue.pop_front();
             }
-            more = !queue_.empty();
+            more = !queue.empty();
         }
-        if (more) cv_work_.notify_one();
+        if (more) cv_work_.notify_all();
         // merge the regions into one batch
         std::vector<int32_t> rpr, hpr, rl, hl;
         std::vector<int64_t> ro, ho;

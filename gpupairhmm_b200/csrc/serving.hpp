@@ -8,6 +8,10 @@
 // completes the tickets.  While one slot's batch runs on the GPU the next slot
 // is already admitting, uploading and launching, so the work of regions that
 // arrive while others are on the device overlaps with them.
+//
+// Regions with reads longer than the largest single tile (multi-tile work,
+// whose pairs each take a long serial wavefront) queue separately and run on
+// their own slot, so that a batch of short regions never waits behind them.
 #pragma once
 
 #include <chrono>
@@ -36,7 +40,8 @@ public:
     pairhmm_status_t latency(uint64_t ticket, double* ms);
     const std::string& last_error() const { return error_; }
 
-    static constexpr int kSlots = 2;
+    static constexpr int kLightSlots = 2;          // regions of single-tile reads
+    static constexpr int kSlots = kLightSlots + 1;  // + one slot for multi-tile regions
 
 private:
     struct Region {
@@ -46,6 +51,7 @@ private:
         std::vector<uint8_t> read_bases, bq, iq, dq, hap_bases;
         int64_t pairs = 0;
         int64_t device_bytes = 0;
+        bool heavy = false;  // has a read beyond the largest single tile
         std::chrono::steady_clock::time_point t_submit, t_done;
         std::vector<float> scores;
         bool done = false;
@@ -62,7 +68,8 @@ private:
     std::vector<std::thread> threads_;
     std::mutex mu_;
     std::condition_variable cv_work_, cv_done_;
-    std::deque<std::shared_ptr<Region>> queue_;
+    std::deque<std::shared_ptr<Region>> light_, heavy_;
+    int32_t single_tile_max_ = 0;  // longest read length without multi-tile work
     std::map<uint64_t, std::shared_ptr<Region>> tickets_;
     uint64_t next_ticket_ = 1;
     bool stop_ = false;

@@ -229,6 +229,16 @@ const char* pairhmm_last_error(const pairhmm_engine_t* engine);
 /* Number of pairs and DP cells of a host batch (gpuworker.cuh:495-520). */
 pairhmm_status_t pairhmm_batch_counts(const pairhmm_batch_t* batch, int64_t* pairs, int64_t* cells);
 
+/*
+ * Page-lock (and release) a caller's host buffer so that pairhmm_compute_host
+ * uploads it by DMA straight from that memory; the buffer must not be freed
+ * or reallocated while registered.  The reference gets the same effect by
+ * allocating its batch vectors page-locked (PinnedAllocator, common.cuh:29-55).
+ * Registering memory that is already page-locked is not an error.
+ */
+pairhmm_status_t pairhmm_host_register(void* ptr, size_t bytes);
+pairhmm_status_t pairhmm_host_unregister(void* ptr);
+
 /* Library version string. */
 const char* pairhmm_version(void);
 
