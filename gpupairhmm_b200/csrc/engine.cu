@@ -97,6 +97,11 @@ Engine::~Engine() {
     if (ev1_) cudaEventDestroy(ev1_);
     if (ev_prep_) cudaEventDestroy(ev_prep_);
     if (ev_fp32_) cudaEventDestroy(ev_fp32_);
+    for (int i = 0; i < kSideStreams; ++i) {
+        if (join_[i]) cudaEventDestroy(join_[i]);
+        if (side_[i]) cudaStreamDestroy(side_[i]);
+    }
+    if (fork_) cudaEventDestroy(fork_);
     if (stream_) cudaStreamDestroy(stream_);
 }
 
@@ -127,6 +132,11 @@ pairhmm_status_t Engine::init() {
     if (prop.major < 10) return fail(PAIRHMM_ERR_UNSUPPORTED, "the kernels are built for sm_100a");
     num_sms_ = prop.multiProcessorCount;
     PHMM_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+    for (int i = 0; i < kSideStreams; ++i) {
+        PHMM_CUDA(cudaStreamCreateWithFlags(&side_[i], cudaStreamNonBlocking));
+        PHMM_CUDA(cudaEventCreateWithFlags(&join_[i], cudaEventDisableTiming));
+    }
+    PHMM_CUDA(cudaEventCreateWithFlags(&fork_, cudaEventDisableTiming));
     PHMM_CUDA(cudaEventCreate(&ev0_));
     PHMM_CUDA(cudaEventCreate(&ev1_));
     PHMM_CUDA(cudaEventCreate(&ev_prep_));
@@ -562,42 +572,58 @@ pairhmm_status_t Engine::enqueue_pipeline(const pairhmm_batch_t& in, const Batch
     v.rescue_enabled = (!plain && opts_.fp64_rescue) ? 1 : 0;
     v.ph2pr = ph2pr_.as<float>();
 
+    // engine form: the stage's launches go round-robin onto the side streams
+    // (forked from s, joined back below); the plain form keeps one stream
+    const bool fork = !plain;
+    int nlaunch = 0;
+    auto next_stream = [&]() { return fork ? side_[nlaunch++ % kSideStreams] : s; };
+    if (fork) {
+        PHMM_CUDA(cudaEventRecord(fork_, s));
+        for (int i = 0; i < kSideStreams; ++i) PHMM_CUDA(cudaStreamWaitEvent(side_[i], fork_, 0));
+    }
     if (stage == 1) {
-    for (int rank = 0; rank < nb; ++rank) {
-        const int b = plain ? rank : nb - 1 - rank;
-        if (x.bucket_items[b] == 0) continue;
-        const ConfigInfo* c = rule_cfg_[b];
-        Fp32LaunchArgs la{};
-        la.view = v;
-        la.items = items_.as<Item>();
-        la.sched = sched_.as<Schedule>();
-        la.rank = rank;
-        la.persistent = plan.persistent[b];
-        la.counter = counters + rank;
-        la.scratch = scratch_.ptr;
-        la.rows = plan.rows;
-        la.grid = plan.grid[b];
-        la.stream = s;
-        PHMM_CUDA(c->launch(la));
-        ++launches_;
+        for (int rank = 0; rank < nb; ++rank) {
+            const int b = plain ? rank : nb - 1 - rank;
+            if (x.bucket_items[b] == 0) continue;
+            const ConfigInfo* c = rule_cfg_[b];
+            Fp32LaunchArgs la{};
+            la.view = v;
+            la.items = items_.as<Item>();
+            la.sched = sched_.as<Schedule>();
+            la.rank = rank;
+            la.persistent = plan.persistent[b];
+            la.counter = counters + rank;
+            la.scratch = static_cast<char*>(scratch_.ptr) + plan.scratch_off[b];
+            la.rows = plan.rows;
+            la.grid = plan.grid[b];
+            la.stream = next_stream();
+            PHMM_CUDA(c->launch(la));
+            ++launches_;
+        }
+    } else {
+        // stage 2: FP64 pass over flagged pairs (FP32 underflow, or degenerate alpha);
+        // only the last class uses the border scratch
+        for (int c = 0; c < kFp64Classes; ++c) {
+            if (x.class_pairs[c] == 0) continue;
+            Fp64LaunchArgs fa{};
+            fa.view = v;
+            fa.cls = c;
+            fa.items = v.rescue[c];
+            fa.count = counters + kMaxBuckets + c;
+            fa.counter = counters + kMaxBuckets + kFp64Classes + c;
+            fa.scratch = scratch_.ptr;
+            fa.rows = plan.rows;
+            fa.grid = plan.fp64_grid[c];
+            fa.stream = next_stream();
+            PHMM_CUDA(launch_fp64_rescue(fa));
+            ++launches_;
+        }
     }
-    return PAIRHMM_OK;
-    }
-    // stage 2: FP64 pass over flagged pairs (FP32 underflow, or degenerate alpha)
-    for (int c = 0; c < kFp64Classes; ++c) {
-        if (x.class_pairs[c] == 0) continue;
-        Fp64LaunchArgs fa{};
-        fa.view = v;
-        fa.cls = c;
-        fa.items = v.rescue[c];
-        fa.count = counters + kMaxBuckets + c;
-        fa.counter = counters + kMaxBuckets + kFp64Classes + c;
-        fa.scratch = scratch_.ptr;
-        fa.rows = plan.rows;
-        fa.grid = plan.fp64_grid[c];
-        fa.stream = s;
-        PHMM_CUDA(launch_fp64_rescue(fa));
-        ++launches_;
+    if (fork) {
+        for (int i = 0; i < kSideStreams; ++i) {
+            PHMM_CUDA(cudaEventRecord(join_[i], side_[i]));
+            PHMM_CUDA(cudaStreamWaitEvent(s, join_[i], 0));
+        }
     }
     return PAIRHMM_OK;
 }
@@ -609,7 +635,14 @@ Engine::Plan Engine::make_plan(const BatchIndex& x) const {
     p.rows = round_up((int64_t)x.max_hap_len + 2 * 32 + 8, 64);
     p.grid.assign(nb, 0);
     p.persistent.assign(nb, 1);
-    int64_t scratch = 0;
+    p.scratch_off.assign(nb, 0);
+    // multi-tile buckets may run at the same time: each gets its own slice of
+    // the border scratch, out of an equal share of the budget
+    int n_mt = 0;
+    for (int b = 0; b < nb; ++b)
+        if (x.bucket_items[b] != 0 && rule_cfg_[b]->multi_tile) ++n_mt;
+    const int64_t mt_budget = kScratchBudget / std::max(1, n_mt);
+    int64_t scratch = 0, fp32_scratch = 0;
     for (int b = 0; b < nb; ++b) {
         if (x.bucket_items[b] == 0) continue;
         const ConfigInfo* c = rule_cfg_[b];
@@ -618,9 +651,10 @@ Engine::Plan Engine::make_plan(const BatchIndex& x) const {
         int64_t grid = plain ? need_blocks : std::min<int64_t>(persistent_grid(c->kernel, c->smem_bytes), need_blocks);
         if (c->multi_tile) {
             const int64_t per_warp = (int64_t)c->scratch_bytes_per_row * p.rows;
-            const int64_t cap_blocks = std::max<int64_t>(1, kScratchBudget / (per_warp * kWarpsPerBlock));
+            const int64_t cap_blocks = std::max<int64_t>(1, mt_budget / (per_warp * kWarpsPerBlock));
             grid = std::min(grid, cap_blocks);
-            scratch = std::max(scratch, grid * kWarpsPerBlock * per_warp);
+            p.scratch_off[b] = fp32_scratch;
+            fp32_scratch += round_up(grid * kWarpsPerBlock * per_warp, 256);
         }
         grid = std::max<int64_t>(1, std::min<int64_t>(grid, INT32_MAX));
         p.grid[b] = (int)grid;
@@ -639,7 +673,7 @@ Engine::Plan Engine::make_plan(const BatchIndex& x) const {
         grid = std::min<int64_t>(grid, std::max<int64_t>(1, (need + kWarpsPerBlock - 1) / kWarpsPerBlock));
         p.fp64_grid[c] = (int)grid;
     }
-    p.scratch_bytes = (size_t)std::max<int64_t>(scratch, 256);
+    p.scratch_bytes = (size_t)std::max<int64_t>(std::max(scratch, fp32_scratch), 256);
     return p;
 }
 

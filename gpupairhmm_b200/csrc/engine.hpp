@@ -91,6 +91,7 @@ private:
         std::vector<int> grid;            // by bucket
         std::vector<int> persistent;      // by bucket
         int fp64_grid[kFp64Classes] = {};   // by FP64 length class
+        std::vector<int64_t> scratch_off;   // by bucket: multi-tile kernels run side by side
         size_t scratch_bytes = 0;
     };
     Plan make_plan(const BatchIndex& idx) const;
@@ -109,6 +110,12 @@ private:
     int num_sms_ = 0;
     bool ready_ = false;
     cudaStream_t stream_ = nullptr;
+    // the launches of one stage (bucket kernels, FP64 classes) fork onto side
+    // streams so that their tails overlap and a small batch's buckets run side
+    // by side; they join back into stream_ before the stage ends
+    static constexpr int kSideStreams = 4;
+    cudaStream_t side_[kSideStreams] = {};
+    cudaEvent_t fork_ = nullptr, join_[kSideStreams] = {};
     cudaEvent_t ev0_ = nullptr, ev1_ = nullptr, ev_prep_ = nullptr, ev_fp32_ = nullptr;
     int64_t launches_ = 0;
     cudaGraphExec_t graph_exec_[3] = {nullptr, nullptr, nullptr};  // prep, FP32, FP64
