@@ -115,6 +115,20 @@ def test_fp64_rescue_of_underflowing_pairs(engine):
     assert_log10_close(got, want, what="cfg2 with rescue")
 
 
+def test_fp64_length_class_boundaries(engine):
+    """Unrelated high-quality reads at every FP64 length-class edge (64, 96,
+    128, 192, 256 single tile, then multi-tile): all of them underflow FP32 and
+    are recomputed by the class's FP64 kernel."""
+    rng = np.random.default_rng(22)
+    recs = [_record(rng, L, 400, n_reads=2, n_haps=2, bq=(35, 42), related=False)
+            for L in [1, 63, 64, 65, 95, 96, 97, 127, 128, 129, 191, 192, 193, 255, 256, 257, 300, 511, 513]]
+    b = _soa(recs)
+    want = oracle.batch_log10(b)
+    got = engine.compute(b)
+    assert engine.stats().rescued >= int((want < -67.0).sum())
+    assert_log10_close(got, want, what="FP64 class boundaries")
+
+
 def test_rescue_disabled_keeps_fp32_results():
     e = g.Engine(fp64_rescue=False)
     b = synth.config2(seed=12, regions=2)
