@@ -16,6 +16,12 @@
 // Values more than 2^1022 below the largest value of their lane are dropped;
 // their contribution to the result is below that factor too.
 //
+// The read-end carry runs with the in-read eps: at position L the I update
+// takes delta = eps*beta, so I there is eps times the carried value, and every
+// position beyond L multiplies by eps once more.  The result lane removes the
+// n = (positions from L to its last register) factors of eps exactly in log
+// space.  One eps for every position keeps no per-position eps registers.
+//
 // The recurrence is the plain one (alpha kept, not divided out), so pairs
 // with alpha ~ 0 are exact here.  Work split as in the FP32 kernel: groups of
 // G lanes, R doubles per lane, T = G*R read positions per tile; reads longer
@@ -75,11 +81,12 @@ struct Fp64Wavefront {
         double acc = 0.0;
         int e = 0;
         int rlane = -1;
+        int ncarry = 0;  // factors of eps on the result lane's carry
 
         for (int tile = 0; tile < ntiles; ++tile) {
             const bool last = tile == ntiles - 1;
             const int p0 = tile * T + t * R;
-            double alpha[R], dlt[R], sig[R], eps[R], M[R], D[R];
+            double alpha[R], dlt[R], sig[R], M[R], D[R];
 #pragma unroll
             for (int q = 0; q < Q; ++q) {
                 double lam[5][2];
@@ -99,9 +106,8 @@ struct Fp64Wavefront {
                     for (int h = 0; h < 5; ++h)
                         lam[h][s] = in ? ((x == 4u || h == 4 || x == (uint32_t)h) ? lm : lx) : 0.0;
                     alpha[r] = (double)(1.0f - (d + sg));
-                    dlt[r] = in ? beta * (double)d : (c == L ? beta : 0.0);
+                    dlt[r] = in ? beta * (double)d : (c == L ? epsd * beta : 0.0);
                     sig[r] = beta * (double)sg;
-                    eps[r] = in ? epsd : 1.0;
                     M[r] = 0.0;
                     D[r] = 0.0;
                 }
@@ -118,7 +124,10 @@ struct Fp64Wavefront {
             const int kg = last ? Hc + t_res : Hc + G - 1;
             const bool res_lane = valid && last && t == t_res;
             const bool addM = r_res == R - 1;
-            if (res_lane) rlane = t;
+            if (res_lane) {
+                rlane = t;
+                ncarry = addM ? 0 : R - 1 - r_res;
+            }
             const int kmax = (int)__reduce_max_sync(kFullMask, (unsigned)(valid ? kg : 0));
             const int K = (kmax + 1 + 3) & ~3;
 
@@ -176,7 +185,7 @@ struct Fp64Wavefront {
                             const double Dold = D[r];
                             M[r] = ls[u] * fma(alpha[r], Mdiag, Xdiag);
                             D[r] = fma(sig[r], Mold, epsd * Dold);
-                            const double In = fma(eps[r], Idiag, dlt[r] * Mdiag);
+                            const double In = fma(epsd, Idiag, dlt[r] * Mdiag);
                             Mdiag = Mold;
                             Idiag = In;
                             Xdiag = In + Dold;
@@ -240,7 +249,7 @@ struct Fp64Wavefront {
             double res = -INFINITY;
             if (acc > 0.0)
                 res = log10(acc) - (double)e * 0.30102999566398119521 - log10((double)kScale) -
-                      log10((double)kBeta);
+                      log10((double)kBeta) - (double)ncarry * log10(epsd);
             v.scores[task.out] = (float)res;
         }
     }
