@@ -62,7 +62,7 @@ cudaError_t DevBuf::ensure(size_t bytes) {
     if (bytes <= cap && ptr) return cudaSuccess;
     release();
     size_t want = std::max<size_t>(bytes + bytes / 4, 256);
-    cudaError_t e = cudaMalloc(&ptr, want);
+    cudaError_t e = pool ? cudaMallocFromPoolAsync(&ptr, want, pool, stream) : cudaMalloc(&ptr, want);
     if (e != cudaSuccess) {
         ptr = nullptr;
         cap = 0;
@@ -73,7 +73,10 @@ cudaError_t DevBuf::ensure(size_t bytes) {
 }
 
 void DevBuf::release() {
-    if (ptr) cudaFree(ptr);
+    if (ptr) {
+        if (pool) cudaFreeAsync(ptr, stream);
+        else cudaFree(ptr);
+    }
     ptr = nullptr;
     cap = 0;
 }
@@ -82,17 +85,22 @@ Engine::Engine(const pairhmm_options_t& opts) : opts_(opts) {
     rules_ = opts_.mode == PAIRHMM_MODE_PLAIN ? plain_rules() : engine_default_rules();
 }
 
+std::vector<DevBuf*> Engine::all_buffers() {
+    return {&ph2pr_, &rules_maxlen_, &rules_rank_, &per_task_, &config_, &in_read_bases_, &in_bq_,
+            &in_iq_, &in_dq_, &in_read_off_, &in_read_len_, &in_hap_bases_, &in_hap_off_, &in_hap_len_,
+            &read_record_, &read_local_, &rec_haps_, &rec_hap_base_, &rec_pair_base_, &read_start_,
+            &hap_start_, &read_pack_, &hap_code_, &hist_, &cursor_, &items_, &rescue_, &counters_,
+            &sched_, &scores_, &scratch_, &lens_tmp_, &unit_read0_, &unit_read1_, &unit_bucket_};
+}
+
 Engine::~Engine() {
     if (ready_) cudaSetDevice(opts_.device);
     for (cudaGraphExec_t& g : graph_exec_)
         if (g) cudaGraphExecDestroy(g);
-    DevBuf* bufs[] = {&ph2pr_, &rules_maxlen_, &rules_rank_, &per_task_, &config_, &in_read_bases_, &in_bq_,
-                      &in_iq_, &in_dq_, &in_read_off_, &in_read_len_, &in_hap_bases_, &in_hap_off_, &in_hap_len_,
-                      &read_record_, &read_local_, &rec_haps_, &rec_hap_base_, &rec_pair_base_, &read_start_,
-                      &hap_start_, &read_pack_, &hap_code_, &hist_, &cursor_, &items_, &rescue_, &counters_,
-                      &sched_, &scores_, &scratch_, &lens_tmp_, &unit_read0_, &unit_read1_, &unit_bucket_};
-    for (DevBuf* b : bufs) b->release();
-    if (host_out_) cudaFreeHost(host_out_);
+    for (DevBuf* b : all_buffers()) b->release();
+    if (stream_) cudaStreamSynchronize(stream_);
+    if (pool_) cudaMemPoolDestroy(pool_);
+    if (host_hdr_) cudaFreeHost(host_hdr_);
     if (ev0_) cudaEventDestroy(ev0_);
     if (ev1_) cudaEventDestroy(ev1_);
     if (ev_prep_) cudaEventDestroy(ev_prep_);
@@ -137,6 +145,20 @@ pairhmm_status_t Engine::init() {
         PHMM_CUDA(cudaEventCreateWithFlags(&join_[i], cudaEventDisableTiming));
     }
     PHMM_CUDA(cudaEventCreateWithFlags(&fork_, cudaEventDisableTiming));
+    {
+        cudaMemPoolProps props{};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = opts_.device;
+        PHMM_CUDA(cudaMemPoolCreate(&pool_, &props));
+        uint64_t keep = UINT64_MAX;
+        PHMM_CUDA(cudaMemPoolSetAttribute(pool_, cudaMemPoolAttrReleaseThreshold, &keep));
+        for (DevBuf* b : all_buffers()) {
+            b->pool = pool_;
+            b->stream = stream_;
+        }
+    }
+    PHMM_CUDA(cudaMallocHost(&host_hdr_, 64));
     PHMM_CUDA(cudaEventCreate(&ev0_));
     PHMM_CUDA(cudaEventCreate(&ev1_));
     PHMM_CUDA(cudaEventCreate(&ev_prep_));
@@ -784,27 +806,16 @@ pairhmm_status_t Engine::compute_host(const pairhmm_batch_t& b, float* scores) {
 
     PHMM_CUDA(cudaEventRecord(ev0_, s));
     if ((st = run_pipeline(dev, x, scores_.as<float>(), s)) != PAIRHMM_OK) return st;
-    // scores go straight into a page-locked caller buffer; otherwise through
-    // this engine's page-locked staging (a copy into pageable memory would
-    // hold the driver's pageable-copy path while it waits for this stream)
-    const bool direct = HostUploader::is_page_locked(scores);
-    const size_t stage_bytes = 64 + (direct ? 0 : 4 * (size_t)x.num_pairs);
-    if (stage_bytes > host_out_cap_) {
-        if (host_out_) cudaFreeHost(host_out_);
-        host_out_ = nullptr;
-        host_out_cap_ = 0;
-        PHMM_CUDA(cudaMallocHost(&host_out_, stage_bytes + stage_bytes / 4));
-        host_out_cap_ = stage_bytes + stage_bytes / 4;
-    }
-    float* dst = direct ? scores : reinterpret_cast<float*>(static_cast<char*>(host_out_) + 64);
-    PHMM_CUDA(cudaMemcpyAsync(dst, scores_.ptr, 4 * x.num_pairs, cudaMemcpyDeviceToHost, s));
+    // scores go straight into a page-locked caller buffer, otherwise through the
+    // uploader's page-locked slots (a copy into pageable memory would hold the
+    // driver's pageable-copy path while it waits for this stream)
     unsigned long long rescued_by_class[kFp64Classes] = {};
-    static_assert(sizeof(rescued_by_class) <= 64, "rescue counts fit the staging header");
-    PHMM_CUDA(cudaMemcpyAsync(host_out_, counters_.as<unsigned long long>() + kMaxBuckets,
+    static_assert(sizeof(rescued_by_class) <= 64, "rescue counts fit the landing spot");
+    PHMM_CUDA(cudaMemcpyAsync(host_hdr_, counters_.as<unsigned long long>() + kMaxBuckets,
                               sizeof(rescued_by_class), cudaMemcpyDeviceToHost, s));
+    PHMM_CUDA(uploader_.download(opts_.device, scores, scores_.ptr, 4 * (size_t)x.num_pairs, s));
     PHMM_CUDA(cudaStreamSynchronize(s));
-    if (!direct) std::memcpy(scores, dst, 4 * (size_t)x.num_pairs);
-    std::memcpy(rescued_by_class, host_out_, sizeof(rescued_by_class));
+    std::memcpy(rescued_by_class, host_hdr_, sizeof(rescued_by_class));
     float ms = 0.f, a = 0.f, b2 = 0.f, c = 0.f;
     PHMM_CUDA(cudaEventElapsedTime(&ms, ev0_, ev1_));
     PHMM_CUDA(cudaEventElapsedTime(&a, ev0_, ev_prep_));

@@ -46,10 +46,16 @@ struct InputRanges {
     int64_t read_min = 0, read_end = 0, hap_min = 0, hap_end = 0;
 };
 
-// Grow-only device buffer.
+// Grow-only device buffer.  With a pool and a stream set (every engine
+// buffer), growth is stream-ordered (cudaFreeAsync + cudaMallocFromPoolAsync
+// on the engine's stream): unlike cudaFree it does not wait for the whole
+// device, so one engine growing its buffers does not stall other engines'
+// work (serving runs several).
 struct DevBuf {
     void* ptr = nullptr;
     size_t cap = 0;
+    cudaMemPool_t pool = nullptr;
+    cudaStream_t stream = nullptr;
     cudaError_t ensure(size_t bytes);
     void release();
     template <class T> T* as() const { return static_cast<T*>(ptr); }
@@ -133,9 +139,12 @@ private:
     // host-to-device uploads (caller inputs, index) and the reused index
     HostUploader uploader_;
     BatchIndex idx_;
-    // page-locked staging for the download: rescue counts, then scores
-    void* host_out_ = nullptr;
-    size_t host_out_cap_ = 0;
+    // page-locked landing spot for the rescue counts
+    void* host_hdr_ = nullptr;
+    // device memory pool of this engine's buffers (kept, not returned to the
+    // system between batches)
+    cudaMemPool_t pool_ = nullptr;
+    std::vector<DevBuf*> all_buffers();
 };
 
 }  // namespace phmm

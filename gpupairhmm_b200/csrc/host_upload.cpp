@@ -82,4 +82,38 @@ cudaError_t HostUploader::run(int device, const std::vector<Copy>& copies, cudaS
     return cudaSuccess;
 }
 
+cudaError_t HostUploader::download(int device, void* dst, const void* src, size_t bytes, cudaStream_t s) {
+    if (bytes == 0) return cudaSuccess;
+    cudaError_t e = cudaSetDevice(device);
+    if (e != cudaSuccess) return e;
+    if (is_page_locked(dst)) {
+        if ((e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, s)) != cudaSuccess) return e;
+        return cudaStreamSynchronize(s);
+    }
+    if ((e = ensure_staging()) != cudaSuccess) return e;
+    constexpr int kSlots = kThreads * kSlotsPerThread;
+    const size_t n = (bytes + kSlotBytes - 1) / kSlotBytes;
+    auto issue = [&](size_t k) -> cudaError_t {
+        const int slot = (int)(k % kSlots);
+        const size_t off = k * kSlotBytes, len = std::min(kSlotBytes, bytes - off);
+        cudaError_t r = cudaEventSynchronize(done_[slot]);  // the slot's earlier use is over
+        if (r == cudaSuccess)
+            r = cudaMemcpyAsync(stage_ + (size_t)slot * kSlotBytes, static_cast<const char*>(src) + off, len,
+                                cudaMemcpyDeviceToHost, s);
+        if (r == cudaSuccess) r = cudaEventRecord(done_[slot], s);
+        return r;
+    };
+    for (size_t k = 0; k < n && k < (size_t)kSlots; ++k)
+        if ((e = issue(k)) != cudaSuccess) return e;
+    for (size_t k = 0; k < n; ++k) {
+        const int slot = (int)(k % kSlots);
+        if ((e = cudaEventSynchronize(done_[slot])) != cudaSuccess) return e;
+        const size_t off = k * kSlotBytes, len = std::min(kSlotBytes, bytes - off);
+        std::memcpy(static_cast<char*>(dst) + off, stage_ + (size_t)slot * kSlotBytes, len);
+        if (k + kSlots < n && (e = issue(k + kSlots)) != cudaSuccess) return e;
+    }
+    staged_ += bytes;
+    return cudaSuccess;
+}
+
 }  // namespace phmm

@@ -7,7 +7,8 @@
 // reuse the slot once its DMA has completed, so the host copies run in
 // parallel with one another and with the DMA of earlier slots.  (A single
 // cudaMemcpyAsync from pageable memory is staged by the driver one piece at a
-// time on the calling thread.)
+// time on the calling thread.)  Downloads use the same slots in the other
+// direction.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -35,6 +36,12 @@ public:
     // byte has been read: the caller may then reuse its host buffers, and work
     // enqueued on s afterwards sees the data.
     cudaError_t run(int device, const std::vector<Copy>& copies, cudaStream_t s);
+
+    // Device-to-host copy of `bytes` after the work already on stream s: one
+    // DMA into a page-locked `dst`, else chunks through the staging slots,
+    // each copied out on the host as soon as its DMA lands.  Returns when dst
+    // holds the data.
+    cudaError_t download(int device, void* dst, const void* src, size_t bytes, cudaStream_t s);
 
     // bytes that went through staging / straight from page-locked memory in the
     // last run
