@@ -230,14 +230,16 @@ def run_binary(args, cfg):
                 vals.append((float(m.group(1)), float(m.group(2))))
     finally:
         os.unlink(path)
-    secs = sum(v[0] for v in vals)
+    # median step: a single batch per process is exposed to one-off host stalls
+    secs = statistics.median(v[0] for v in vals) * len(vals)
     value = batch.cells() * len(vals) / secs / 1e9
     print(json.dumps({"impl": args.impl, "metric": METRIC, "value": round(value, 3), "unit": "GCUPS",
                       "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
                       "ms_per_step": round(secs / len(vals) * 1e3, 3), "higher_is_better": True,
                       "data": "synthetic", "config": dict(cfg, pairs=batch.num_pairs, cells=batch.cells()),
                       "timing": "the binary's own batch wall clock (upload, kernels, download; file "
-                                "parsing excluded), whole batch at once"}), flush=True)
+                                "parsing excluded), whole batch at once; median over the steps",
+                      "step_seconds": [round(v[0], 4) for v in vals]}), flush=True)
 
 
 def percentile(xs, q):
@@ -391,15 +393,18 @@ def run_ours(args, cfg, rank, world, local_rank):
                                                "fp32": round(fp32_ms / args.steps, 3),
                                                "fp64": round(fp64_ms / args.steps, 3)}},
             "clocks": clocks,
-            "accuracy": accuracy(batch, scores, args.accuracy_pairs, rng),
         }
+        # the streaming-service run goes first: after the OpenMP oracle has run in
+        # this process (accuracy sample, CPU baseline) the serving threads saw
+        # periodic host stalls of several hundred ms
+        if world == 1 and args.serving_seconds > 0:
+            line["serving"] = run_serving(args, local_rank)
+        line["accuracy"] = accuracy(batch, scores, args.accuracy_pairs, rng)
         if world == 1 and not args.no_cpu_baseline:
             import oracle
             gc, desc = cpu_rate(lambda b: oracle.batch_log10(b), batch, args.cpu_seconds, rng)
             line["cpu_baseline"] = {"value": round(gc, 4), "unit": "GCUPS", "cores": os.cpu_count() or 1,
                                     "kind": "port", "sample": desc + "; FP64 oracle, OpenMP over pairs"}
-        if world == 1 and args.serving_seconds > 0:
-            line["serving"] = run_serving(args, local_rank)
         print(json.dumps(line), flush=True)
     engine.close()
     if dist:

@@ -63,6 +63,7 @@ struct PipelineData {
         reg(b.read_lengths.data(), 4 * b.read_lengths.size());
         reg(b.hap_offsets.data(), 8 * b.hap_offsets.size());
         reg(b.hap_lengths.data(), 4 * b.hap_lengths.size());
+        reg(scores.data(), 4 * scores.size());
     }
     void unpin() {
         for (void* p : pinned) pairhmm_host_unregister(p);
@@ -108,6 +109,7 @@ void parser_thread(const Options& o, Queue<PipelineData*>* in, Queue<PipelineDat
         d->batch.clear();
         bool eof = false;
         if (!reader.next(d->batch, o.fileBatchsize, eof)) die("parse error: " + reader.error());
+        d->scores.resize((size_t)std::max<int64_t>(d->batch.pairs, 1));
         d->pin();
         if (d->batch.num_records() > 0) out->push(d);
         else in->push(d);
@@ -140,8 +142,7 @@ void gpu_thread(const Options& o, Queue<PipelineData*>* in, Queue<PipelineData*>
         PipelineData* d = in->pop();
         if (!d) break;
         const auto t0 = std::chrono::steady_clock::now();
-        phmm::HostBatch& b = d->batch;
-        d->scores.resize((size_t)std::max<int64_t>(b.pairs, 1));
+        phmm::HostBatch& b = d->batch;  // scores were sized (and page-locked) by the parser
         // transfer chunks: consecutive records with at least transferBatchsize pairs
         int64_t g = 0, read0 = 0, hap0 = 0, pair0 = 0;
         const int64_t ng = b.num_records();

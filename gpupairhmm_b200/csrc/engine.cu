@@ -776,10 +776,10 @@ pairhmm_status_t Engine::compute_host(const pairhmm_batch_t& b, float* scores) {
         {in_hap_off_.ptr, b.hap_offsets, (size_t)(8 * rg.num_haps)},
         {in_hap_len_.ptr, b.hap_lengths, (size_t)(4 * rg.num_haps)},
     };
-    cudaError_t up = cudaSuccess;
-    std::thread uploader([&] { up = uploader_.run(opts_.device, inputs, s); });
+    cudaError_t up = uploader_.start(opts_.device, inputs, s);
     st = build_index(b, rules_, idx_, err);
-    uploader.join();
+    const cudaError_t upf = uploader_.finish();
+    if (up == cudaSuccess) up = upf;
     if (up != cudaSuccess) return cuda_fail(up, "input upload");
     if (st != PAIRHMM_OK) return fail(st, err);
     const BatchIndex& x = idx_;

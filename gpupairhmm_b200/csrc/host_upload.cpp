@@ -7,6 +7,12 @@
 namespace phmm {
 
 HostUploader::~HostUploader() {
+    {
+        std::lock_guard<std::mutex> lk(mu_);
+        stop_ = true;
+    }
+    cv_work_.notify_all();
+    for (std::thread& th : workers_) th.join();
     for (cudaEvent_t& e : done_)
         if (e) cudaEventDestroy(e);
     if (stage_) cudaFreeHost(stage_);
@@ -32,16 +38,47 @@ cudaError_t HostUploader::ensure_staging() {
     return cudaSuccess;
 }
 
-cudaError_t HostUploader::run(int device, const std::vector<Copy>& copies, cudaStream_t s) {
+void HostUploader::worker_loop(int t) {
+    unsigned long long seen = 0;
+    for (;;) {
+        {
+            std::unique_lock<std::mutex> lk(mu_);
+            cv_work_.wait(lk, [&] { return stop_ || job_ != seen; });
+            if (stop_) return;
+            seen = job_;
+        }
+        copy_pieces(t);
+        {
+            std::lock_guard<std::mutex> lk(mu_);
+            --busy_;
+        }
+        cv_done_.notify_all();
+    }
+}
+
+// copy thread t takes pieces t, t + kThreads, ... through its two slots
+void HostUploader::copy_pieces(int t) {
+    cudaError_t r = cudaSetDevice(device_);
+    int j = 0;
+    for (size_t k = (size_t)t; k < pieces_.size() && r == cudaSuccess; k += kThreads, ++j) {
+        const int slot = t * kSlotsPerThread + (j % kSlotsPerThread);
+        char* buf = stage_ + (size_t)slot * kSlotBytes;
+        // the slot's previous DMA (this job or an earlier one) must be done
+        if ((r = cudaEventSynchronize(done_[slot])) != cudaSuccess) break;
+        std::memcpy(buf, pieces_[k].src, pieces_[k].bytes);
+        if ((r = cudaMemcpyAsync(pieces_[k].dst, buf, pieces_[k].bytes, cudaMemcpyHostToDevice, stream_)) !=
+            cudaSuccess)
+            break;
+        r = cudaEventRecord(done_[slot], stream_);
+    }
+    err_[t] = r;
+}
+
+cudaError_t HostUploader::start(int device, const std::vector<Copy>& copies, cudaStream_t s) {
     staged_ = direct_ = 0;
+    pieces_.clear();
     cudaError_t e = cudaSetDevice(device);
     if (e != cudaSuccess) return e;
-    struct Piece {
-        char* dst;
-        const char* src;
-        size_t bytes;
-    };
-    std::vector<Piece> pieces;
     for (const Copy& c : copies) {
         if (c.bytes == 0) continue;
         if (is_page_locked(c.src)) {
@@ -50,35 +87,38 @@ cudaError_t HostUploader::run(int device, const std::vector<Copy>& copies, cudaS
             continue;
         }
         for (size_t off = 0; off < c.bytes; off += kSlotBytes)
-            pieces.push_back({static_cast<char*>(c.dst) + off, static_cast<const char*>(c.src) + off,
-                              std::min(kSlotBytes, c.bytes - off)});
+            pieces_.push_back({static_cast<char*>(c.dst) + off, static_cast<const char*>(c.src) + off,
+                               std::min(kSlotBytes, c.bytes - off)});
         staged_ += c.bytes;
     }
-    if (pieces.empty()) return cudaSuccess;
-    if ((e = ensure_staging()) != cudaSuccess) return e;
-    const int nthreads = (int)std::min<size_t>(kThreads, pieces.size());
-    cudaError_t err[kThreads] = {};
-    auto worker = [&](int t) {
-        cudaError_t r = cudaSetDevice(device);
-        int j = 0;
-        for (size_t k = (size_t)t; k < pieces.size() && r == cudaSuccess; k += (size_t)nthreads, ++j) {
-            const int slot = t * kSlotsPerThread + (j % kSlotsPerThread);
-            char* buf = stage_ + (size_t)slot * kSlotBytes;
-            // the slot's previous DMA (this run or an earlier one) must be done
-            if ((r = cudaEventSynchronize(done_[slot])) != cudaSuccess) break;
-            std::memcpy(buf, pieces[k].src, pieces[k].bytes);
-            if ((r = cudaMemcpyAsync(pieces[k].dst, buf, pieces[k].bytes, cudaMemcpyHostToDevice, s)) != cudaSuccess)
-                break;
-            r = cudaEventRecord(done_[slot], s);
-        }
-        err[t] = r;
-    };
-    std::vector<std::thread> threads;
-    for (int t = 1; t < nthreads; ++t) threads.emplace_back(worker, t);
-    worker(0);
-    for (std::thread& th : threads) th.join();
-    for (int t = 0; t < nthreads; ++t)
-        if (err[t] != cudaSuccess) return err[t];
+    if (pieces_.empty()) return cudaSuccess;
+    if ((e = ensure_staging()) != cudaSuccess) {
+        pieces_.clear();
+        return e;
+    }
+    if (workers_.empty())
+        for (int t = 0; t < kThreads; ++t) workers_.emplace_back(&HostUploader::worker_loop, this, t);
+    device_ = device;
+    stream_ = s;
+    {
+        std::lock_guard<std::mutex> lk(mu_);
+        for (cudaError_t& x : err_) x = cudaSuccess;
+        busy_ = kThreads;
+        ++job_;
+    }
+    cv_work_.notify_all();
+    return cudaSuccess;
+}
+
+cudaError_t HostUploader::finish() {
+    if (pieces_.empty()) return cudaSuccess;
+    {
+        std::unique_lock<std::mutex> lk(mu_);
+        cv_done_.wait(lk, [&] { return busy_ == 0; });
+    }
+    pieces_.clear();
+    for (cudaError_t x : err_)
+        if (x != cudaSuccess) return x;
     return cudaSuccess;
 }
 

@@ -121,6 +121,12 @@ pairhmm_status_t ServingQueue::submit(const pairhmm_batch_t& b, uint64_t* ticket
 void ServingQueue::worker(int slot) {
     Engine& eng = *engines_[slot];
     std::deque<std::shared_ptr<Region>>& queue = slot < kLightSlots ? light_ : heavy_;
+    // merge buffers live as long as the slot: a batch maps no new memory once
+    // they have grown to the slot's usual size
+    std::vector<int32_t> rpr, hpr, rl, hl;
+    std::vector<int64_t> ro, ho;
+    std::vector<uint8_t> rb, bq, iq, dq, hb;
+    std::vector<float> scores;
     for (;;) {
         std::vector<std::shared_ptr<Region>> take;
         bool more = false;
@@ -143,9 +149,10 @@ void ServingQueue::worker(int slot) {
         }
         if (more) cv_work_.notify_all();
         // merge the regions into one batch
-        std::vector<int32_t> rpr, hpr, rl, hl;
-        std::vector<int64_t> ro, ho;
-        std::vector<uint8_t> rb, bq, iq, dq, hb;
+        for (auto* v : {&rpr, &hpr, &rl, &hl}) v->clear();
+        ro.clear();
+        ho.clear();
+        for (auto* v : {&rb, &bq, &iq, &dq, &hb}) v->clear();
         for (const auto& r : take) {
             const int64_t rbase = (int64_t)rb.size(), hbase = (int64_t)hb.size();
             rpr.insert(rpr.end(), r->rpr.begin(), r->rpr.end());
@@ -175,7 +182,7 @@ void ServingQueue::worker(int slot) {
         b.hap_lengths = hl.data();
         int64_t total_pairs = 0;
         for (const auto& r : take) total_pairs += r->pairs;
-        std::vector<float> scores((size_t)std::max<int64_t>(total_pairs, 1));
+        scores.resize((size_t)std::max<int64_t>(total_pairs, 1));
         const pairhmm_status_t st = eng.compute_host(b, scores.data());
         const auto now = std::chrono::steady_clock::now();
         {
