@@ -72,7 +72,8 @@ struct DevView {
     const int64_t* hap_start;  // in bytes, multiple of 16
     const int32_t* hap_len;
     float* scores;
-    Task* rescue[6];            // flagged pairs by read-length class (fp64_class)
+    Task* rescue_base;          // flagged pairs, one list per read-length class (fp64_class)
+    const long long* rescue_off;  // [kFp64Classes] start of each class list in rescue_base
     unsigned long long* rescue_count;  // [kFp64Classes]
     int rescue_enabled;
     const float* ph2pr;         // 128 floats in global memory
@@ -86,21 +87,18 @@ __device__ __forceinline__ uint32_t code_of(uint8_t c) {
 __device__ __forceinline__ int min_i(int a, int b) { return a < b ? a : b; }
 
 // FP64 pass length classes (tile = G x R): 64 = 8x8, 96 = 16x6, 128 = 16x8,
-// 192 = 32x6, 256 = 32x8, then 32x8 multi-tile for longer reads.
-constexpr int kFp64Classes = 6;
-constexpr int kFp64ClassMax[kFp64Classes - 1] = {64, 96, 128, 192, 256};
+// 160 = 16x10, 192 = 32x6, 256 = 32x8, then 32x8 multi-tile for longer reads.
+constexpr int kFp64Classes = 7;
+constexpr int kFp64ClassMax[kFp64Classes - 1] = {64, 96, 128, 160, 192, 256};
 __host__ __device__ __forceinline__ int fp64_class(int L) {
-    return L <= 64 ? 0 : L <= 96 ? 1 : L <= 128 ? 2 : L <= 192 ? 3 : L <= 256 ? 4 : 5;
+    return L <= 64 ? 0 : L <= 96 ? 1 : L <= 128 ? 2 : L <= 160 ? 3 : L <= 192 ? 4 : L <= 256 ? 5 : 6;
 }
 
-// Appends a flagged pair to its FP64 class list.  The list pointer is picked
-// with constant indices: a run-time index into the kernel-parameter array would
-// copy the whole parameter block to local memory.
+// Appends a flagged pair to its FP64 class list (rare: one global load for the
+// list start).
 __device__ __forceinline__ void append_rescue(const DevView& v, int cls, const Task& t) {
-    Task* dst = cls == 0 ? v.rescue[0] : cls == 1 ? v.rescue[1] : cls == 2 ? v.rescue[2]
-              : cls == 3 ? v.rescue[3] : cls == 4 ? v.rescue[4] : v.rescue[5];
     const unsigned long long slot = atomicAdd(v.rescue_count + cls, 1ull);
-    dst[slot] = t;
+    v.rescue_base[v.rescue_off[cls] + (long long)slot] = t;
 }
 
 }  // namespace phmm

@@ -90,7 +90,7 @@ std::vector<DevBuf*> Engine::all_buffers() {
             &in_iq_, &in_dq_, &in_read_off_, &in_read_len_, &in_hap_bases_, &in_hap_off_, &in_hap_len_,
             &read_record_, &read_local_, &rec_haps_, &rec_hap_base_, &rec_pair_base_, &read_start_,
             &hap_start_, &read_pack_, &hap_code_, &hist_, &cursor_, &items_, &rescue_, &counters_,
-            &sched_, &scores_, &scratch_, &lens_tmp_, &unit_read0_, &unit_read1_, &unit_bucket_};
+            &sched_, &scores_, &scratch_, &lens_tmp_, &unit_read0_, &unit_read1_, &unit_bucket_, &rescue_off_};
 }
 
 Engine::~Engine() {
@@ -238,6 +238,7 @@ pairhmm_status_t Engine::build_index(const pairhmm_batch_t& b, const std::vector
     x.pack_positions = x.code_bytes = 0;
     x.multi_tile_pairs = 0;
     for (int64_t& c : x.class_pairs) c = 0;
+    for (int64_t& c : x.class_start) c = 0;
     x.unit_read0.clear();
     x.unit_read1.clear();
     x.unit_bucket.clear();
@@ -375,6 +376,13 @@ pairhmm_status_t Engine::build_index(const pairhmm_batch_t& b, const std::vector
             }
         x.cells += sl * rec_hap_sum[g];
     }
+    {
+        int64_t off = 0;
+        for (int c = 0; c < kFp64Classes; ++c) {
+            x.class_start[c] = off;
+            off += x.class_pairs[c];
+        }
+    }
     return PAIRHMM_OK;
 }
 
@@ -473,6 +481,7 @@ pairhmm_status_t Engine::ensure_buffers(const BatchIndex& x, bool host_inputs) {
     PHMM_CUDA(cursor_.ensure(8 * nbins));
     PHMM_CUDA(items_.ensure(sizeof(Item) * np));
     PHMM_CUDA(rescue_.ensure(sizeof(Task) * np));  // class lists laid out back to back
+    PHMM_CUDA(rescue_off_.ensure(sizeof(int64_t) * kFp64Classes));
     return PAIRHMM_OK;
 }
 
@@ -488,6 +497,7 @@ pairhmm_status_t Engine::upload_index(const BatchIndex& x, cudaStream_t s) {
         {unit_read0_.ptr, x.unit_read0.data(), 4 * x.unit_read0.size()},
         {unit_read1_.ptr, x.unit_read1.data(), 4 * x.unit_read1.size()},
         {unit_bucket_.ptr, x.unit_bucket.data(), 4 * x.unit_bucket.size()},
+        {rescue_off_.ptr, x.class_start, sizeof(x.class_start)},
     };
     PHMM_CUDA(uploader_.run(opts_.device, copies, s));
     return PAIRHMM_OK;
@@ -583,13 +593,8 @@ pairhmm_status_t Engine::enqueue_pipeline(const pairhmm_batch_t& in, const Batch
     v.hap_start = pa.hap_start;
     v.hap_len = in.hap_lengths;
     v.scores = d_scores;
-    {
-        int64_t off = 0;
-        for (int c = 0; c < kFp64Classes; ++c) {
-            v.rescue[c] = rescue_.as<Task>() + off;
-            off += x.class_pairs[c];
-        }
-    }
+    v.rescue_base = rescue_.as<Task>();
+    v.rescue_off = rescue_off_.as<long long>();
     v.rescue_count = counters + kMaxBuckets;
     v.rescue_enabled = (!plain && opts_.fp64_rescue) ? 1 : 0;
     v.ph2pr = ph2pr_.as<float>();
@@ -630,7 +635,7 @@ pairhmm_status_t Engine::enqueue_pipeline(const pairhmm_batch_t& in, const Batch
             Fp64LaunchArgs fa{};
             fa.view = v;
             fa.cls = c;
-            fa.items = v.rescue[c];
+            fa.items = rescue_.as<Task>() + x.class_start[c];
             fa.count = counters + kMaxBuckets + c;
             fa.counter = counters + kMaxBuckets + kFp64Classes + c;
             fa.scratch = scratch_.ptr;

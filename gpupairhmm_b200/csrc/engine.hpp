@@ -36,6 +36,7 @@ struct BatchIndex {
     std::vector<int64_t> bucket_items;              // work items (unit x haplotype) by bucket
     std::vector<int32_t> unit_read0, unit_read1, unit_bucket;  // units: 1 or 2 reads of a record
     int64_t class_pairs[kFp64Classes] = {};         // by FP64 length class (fp64_class)
+    int64_t class_start[kFp64Classes] = {};         // start of each class's FP64 list
     int64_t multi_tile_pairs = 0;
 };
 
@@ -135,7 +136,7 @@ private:
     DevBuf read_record_, read_local_, rec_haps_, rec_hap_base_, rec_pair_base_, read_start_, hap_start_;
     DevBuf unit_read0_, unit_read1_, unit_bucket_;
     DevBuf read_pack_, hap_code_, hist_, cursor_, items_, rescue_, counters_, sched_, scores_, scratch_;
-    DevBuf lens_tmp_;
+    DevBuf lens_tmp_, rescue_off_;
     // host-to-device uploads (caller inputs, index) and the reused index
     HostUploader uploader_;
     BatchIndex idx_;

@@ -17,8 +17,15 @@ namespace phmm {
 template <int G, int R, bool MT, bool PK>
 using WavefrontOf = typename std::conditional<PK, Fp32x2Wavefront<G, R>, Fp32Wavefront<G, R, MT>>::type;
 
+// Resident CTAs per SM asked of the register allocator for configurations whose
+// natural allocation sits just above an occupancy step (64-thread CTAs: 6 CTAs
+// at <= 170 registers); 1 leaves the allocator free.
+constexpr int fp32_min_ctas(int R, bool MT, bool PK) {
+    return PK ? (R <= 8 ? 6 : 1) : (!MT && R <= 20 ? 6 : 1);
+}
+
 template <int G, int R, bool MT, bool PK>
-__global__ void __launch_bounds__(kBlockThreads)
+__global__ void __launch_bounds__(kBlockThreads, fp32_min_ctas(R, MT, PK))
 fp32_bucket_kernel(DevView v, const Item* __restrict__ items, const Schedule* __restrict__ s, int rank,
                    int persistent, unsigned long long* counter, float4* scratch, int64_t rows) {
     static_assert(!(MT && PK), "the packed kernel is single tile");

@@ -37,11 +37,12 @@ const ConfigInfo* find_fp32_config(int G, int R, bool multi_tile, bool packed) {
 using W64c0 = Fp64Wavefront<8, 8, false>;
 using W64c1 = Fp64Wavefront<16, 6, false>;
 using W64c2 = Fp64Wavefront<16, 8, false>;
-using W64c3 = Fp64Wavefront<32, 6, false>;
-using W64c4 = Fp64Wavefront<32, 8, false>;
-using W64c5 = Fp64Wavefront<32, 8, true>;
+using W64c3 = Fp64Wavefront<16, 10, false>;
+using W64c4 = Fp64Wavefront<32, 6, false>;
+using W64c5 = Fp64Wavefront<32, 8, false>;
+using W64c6 = Fp64Wavefront<32, 8, true>;
 static_assert(W64c0::T == kFp64ClassMax[0] && W64c1::T == kFp64ClassMax[1] && W64c2::T == kFp64ClassMax[2] &&
-                  W64c3::T == kFp64ClassMax[3] && W64c4::T == kFp64ClassMax[4],
+                  W64c3::T == kFp64ClassMax[3] && W64c4::T == kFp64ClassMax[4] && W64c5::T == kFp64ClassMax[5],
               "class bounds follow the tiles");
 
 template <class W>
@@ -85,7 +86,8 @@ size_t fp64_smem_for() {
         case 2: { using W = W64c2; EXPR; }  \
         case 3: { using W = W64c3; EXPR; }  \
         case 4: { using W = W64c4; EXPR; }  \
-        default: { using W = W64c5; EXPR; } \
+        case 5: { using W = W64c5; EXPR; }  \
+        default: { using W = W64c6; EXPR; } \
     }
 
 size_t fp64_smem_bytes(int cls) { PHMM_FP64_DISPATCH(cls, return fp64_smem_for<W>()); }

@@ -46,7 +46,17 @@ struct PrepArgs {
 };
 
 #ifdef PHMM_PREP_KERNELS_IMPL
-// warp per read
+__device__ __forceinline__ uint32_t pack_position(uint32_t base, uint32_t bq, uint32_t iq, uint32_t dq) {
+    bq = bq > 127u ? 127u : bq;
+    iq = iq > 127u ? 127u : iq;
+    dq = dq > 127u ? 127u : dq;
+    return code_of((uint8_t)base) | (bq << 8) | (iq << 16) | (dq << 24);
+}
+
+// Warp per read; a lane packs 4 consecutive positions and stores them as one
+// 16-byte word group.  Where the four source arrays are 4-byte aligned at the
+// read's offset, whole groups inside the read are read with one 4-byte load
+// per array; the read's ragged end (and unaligned sources) go byte by byte.
 __global__ void pack_reads_kernel(PrepArgs a) {
     const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
@@ -55,23 +65,38 @@ __global__ void pack_reads_kernel(PrepArgs a) {
         const int L = a.read_lengths[i];
         const int Lp = (L + 3) & ~3;
         const int64_t src = a.read_offsets[i];
-        uint32_t* dst = a.read_pack + a.read_start[i];
-        for (int c = lane; c < Lp; c += 32) {
-            uint32_t w = 4u;
-            if (c < L) {
-                const uint32_t x = code_of(a.read_bases[src + c]);
-                uint32_t bq = a.base_quals[src + c], iq = a.ins_quals[src + c], dq = a.del_quals[src + c];
-                bq = bq > 127u ? 127u : bq;
-                iq = iq > 127u ? 127u : iq;
-                dq = dq > 127u ? 127u : dq;
-                w = x | (bq << 8) | (iq << 16) | (dq << 24);
+        const uint8_t* rb = a.read_bases + src;
+        const uint8_t* bq = a.base_quals + src;
+        const uint8_t* iq = a.ins_quals + src;
+        const uint8_t* dq = a.del_quals + src;
+        const bool aligned = ((reinterpret_cast<uintptr_t>(rb) | reinterpret_cast<uintptr_t>(bq) |
+                               reinterpret_cast<uintptr_t>(iq) | reinterpret_cast<uintptr_t>(dq)) & 3u) == 0;
+        uint4* dst = reinterpret_cast<uint4*>(a.read_pack + a.read_start[i]);  // 16-byte aligned
+        for (int c = lane * 4; c < Lp; c += 128) {
+            uint32_t w[4];
+            if (aligned && c + 3 < L) {
+                const uint32_t r4 = *reinterpret_cast<const uint32_t*>(rb + c);
+                const uint32_t b4 = *reinterpret_cast<const uint32_t*>(bq + c);
+                const uint32_t i4 = *reinterpret_cast<const uint32_t*>(iq + c);
+                const uint32_t d4 = *reinterpret_cast<const uint32_t*>(dq + c);
+#pragma unroll
+                for (int j = 0; j < 4; ++j)
+                    w[j] = pack_position((r4 >> (8 * j)) & 0xffu, (b4 >> (8 * j)) & 0xffu, (i4 >> (8 * j)) & 0xffu,
+                                         (d4 >> (8 * j)) & 0xffu);
+            } else {
+#pragma unroll
+                for (int j = 0; j < 4; ++j)
+                    w[j] = c + j < L ? pack_position(rb[c + j], bq[c + j], iq[c + j], dq[c + j]) : 4u;
             }
-            dst[c] = w;
+            dst[c >> 2] = make_uint4(w[0], w[1], w[2], w[3]);
         }
     }
 }
 
-// warp per haplotype; pads to 16 bytes with code 4
+// Warp per haplotype; a lane encodes 16 consecutive positions (4-byte loads
+// where the source is 4-byte aligned and the 16 positions are inside the
+// haplotype) and stores them as one 16-byte word; the padding to 16 bytes is
+// code 4.
 __global__ void pack_haps_kernel(PrepArgs a) {
     const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
@@ -79,9 +104,32 @@ __global__ void pack_haps_kernel(PrepArgs a) {
     for (int64_t i = warp; i < a.num_haps; i += nwarps) {
         const int H = a.hap_lengths[i];
         const int Hp = (H + 15) & ~15;
-        const int64_t src = a.hap_offsets[i];
-        uint8_t* dst = a.hap_code + a.hap_start[i];
-        for (int c = lane; c < Hp; c += 32) dst[c] = c < H ? (uint8_t)code_of(a.hap_bases[src + c]) : (uint8_t)4;
+        const uint8_t* hb = a.hap_bases + a.hap_offsets[i];
+        const bool aligned = (reinterpret_cast<uintptr_t>(hb) & 3u) == 0;
+        uint4* dst = reinterpret_cast<uint4*>(a.hap_code + a.hap_start[i]);  // 16-byte aligned
+        for (int c = lane * 16; c < Hp; c += 512) {
+            uint32_t w[4];
+            if (aligned && c + 15 < H) {
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    const uint32_t v = *reinterpret_cast<const uint32_t*>(hb + c + 4 * q);
+                    w[q] = code_of(v & 0xffu) | (code_of((v >> 8) & 0xffu) << 8) | (code_of((v >> 16) & 0xffu) << 16) |
+                           (code_of(v >> 24) << 24);
+                }
+            } else {
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    uint32_t v = 0;
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) {
+                        const int cc = c + 4 * q + j;
+                        v |= (cc < H ? code_of(hb[cc]) : 4u) << (8 * j);
+                    }
+                    w[q] = v;
+                }
+            }
+            dst[c >> 4] = make_uint4(w[0], w[1], w[2], w[3]);
+        }
     }
 }
 
