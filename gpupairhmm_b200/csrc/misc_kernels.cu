@@ -106,8 +106,14 @@ cudaError_t launch_fp64_rescue(const Fp64LaunchArgs& a) {
 
 // ---------------------------------------------------------------- preparation
 cudaError_t launch_pack(const PrepArgs& a, int grid, cudaStream_t s) {
-    pack_reads_kernel<<<grid, 256, 0, s>>>(a);
-    pack_haps_kernel<<<grid, 256, 0, s>>>(a);
+    // a warp per read / haplotype with every warp resident at once where the batch
+    // allows: each warp's work is short, so latency is hidden by warps in flight
+    auto warps_grid = [&](int64_t n) {
+        const int64_t g = (n + 7) / 8;  // 8 warps per 256-thread block
+        return (int)std::max<int64_t>(grid, std::min<int64_t>(g, int64_t(1) << 20));
+    };
+    pack_reads_kernel<<<warps_grid(a.num_reads), 256, 0, s>>>(a);
+    pack_haps_kernel<<<warps_grid(a.num_haps), 256, 0, s>>>(a);
     return cudaGetLastError();
 }
 
