@@ -17,18 +17,29 @@
 //     N(j,c)  = lam'(h_j,c) * (N(j-1,c-1) + It(j-1,c-1) + Dt(j-1,c-1)),  lam' = alpha_{c+1}*lambda
 //     It(j,c) = d'_c*N(j,c-1) + eps_c*It(j,c-1),                        d'   = beta*delta_c/alpha_c
 //     Dt(j,c) = s'_c*N(j-1,c) + eps*Dt(j-1,c),                          s'   = beta*sigma_c/alpha_{c+1}
-// 7 FP32 instructions per cell (FADD+FADD+FMUL, FMUL+FFMA, FMUL+FFMA), only
-// lam' (4 bytes per cell) comes from shared memory, and the per-position
-// registers are N, Dt, d', s', eps (5R).  Pairs with |alpha| < 2^-8 somewhere
-// (ins+del quality around 3 or below) cannot use the division; they are
-// flagged for the FP64 pass, which runs the untransformed recurrence.
-// I is computed one anti-diagonal behind M, as in the reference
-// (pairhmm_kernels.cuh:1423-1426).
+// and each of It and Dt divided by its own per-position input weight, so that
+// the term that feeds it has weight 1 and folds into an FFMA:
+//     I^ = It/q_c  (q_c = d'_c inside the read, beta from the read end on),
+//     D^ = Dt/s'_c,  X^ = (It + Dt(j-1))/q_c  (the diagonal sum N needs):
+//     D^(j,c) = eps*D^(j-1,c) + N(j-1,c)                        FFMA
+//     I^(j,c) = e_c*I^(j,c-1) + N(j-1,c-1)                      FFMA  e_c = eps_c*q_{c-1}/q_c
+//     X^(j,c) = r_c*D^(j-1,c) + I^(j,c)                         FFMA  r_c = s'_c/q_c
+//     N(j,c)  = lam'(h_j,c) * (q_{c-1}*X^(j,c-1) + N(j-1,c-1))   FFMA + FMUL
+// Five FP32 instructions per cell (four FFMA, one FMUL), only lam' (4 bytes
+// per cell) from shared memory, and per-position registers N, D^, q_{c-1},
+// e, r (5R).  The rescaled values stay on the scale of N (q and s' are the
+// weights of what feeds them), so the FP32 range is that of the unscaled
+// form.  Pairs with |alpha| < 2^-8 somewhere (ins+del quality around 3 or
+// below) cannot use the division; they are flagged for the FP64 pass, which
+// runs the untransformed recurrence.  I is computed one anti-diagonal behind
+// M, as in the reference (pairhmm_kernels.cuh:1423-1426).
 //
-// Result: the position after the read end gets alpha = 1, d' = beta, eps = 1
-// and later positions d' = 0, eps = 1, so the lane's last It carries
-// beta*(M+I)(j, L-1) (the reference's trick, pairhmm_kernels.cuh:1307-1331,
-// with beta folded in).  Summing over j gives beta * sum_j (M+I)(L-1,j).
+// Result: positions from the read end on take eps = 1 and the scale q = beta
+// (so N(j-1, L-1) enters I at L with weight beta and later positions only
+// carry); beta times the lane's last I^ is then beta*(M+I)(j, L-1) (the
+// reference's trick, pairhmm_kernels.cuh:1307-1331, with beta folded in).
+// When the read ends on a lane's last position the lane adds q*I^ + beta*N.
+// Summing over j gives beta * sum_j (M+I)(L-1,j).
 //
 // lam' table: each thread owns 5 x R floats in shared memory, laid out as
 // [hap code][R/4][32 lanes] float4, so a warp-wide 16-byte load touches 32
@@ -36,7 +47,7 @@
 // thread only reads what it wrote (no synchronisation).
 //
 // Reads longer than T (MT = true) run as several tiles; the last lane of tile
-// i writes (N, Dt, It) of its last position for every haplotype row into a
+// i writes (X^, I^, N) of its last position for every haplotype row into a
 // per-group scratch border, which lane 0 of tile i+1 reads as its left
 // boundary (pairhmm_kernels.cuh:2167-3272 does the same with 512-row tiles).
 #pragma once
@@ -97,7 +108,18 @@ struct Fp32Wavefront {
                     alpha_next = 1.0f - (ph[(wn >> 16) & 0x7fu] + ph[(wn >> 24) & 0x7fu]);
                 }
             }
-            float dlt[R], sig[R], eps[R];
+            // I scale of the position before this lane's first: 1 at the read's
+            // column -1 (boundary values enter unscaled)
+            float q_prev = 1.0f;
+            if (p0 > 0) {
+                q_prev = kBeta;
+                if (p0 - 1 < L) {
+                    const uint32_t wp = __ldg(rpack + p0 - 1);
+                    const float dp = ph[(wp >> 16) & 0x7fu];
+                    q_prev = (kBeta * dp) / (1.0f - (dp + ph[(wp >> 24) & 0x7fu]));
+                }
+            }
+            float dpv[R], ee[R], rr[R];
             float N[R], D[R];
             float a_cur[R];
 #pragma unroll
@@ -113,6 +135,7 @@ struct Fp32Wavefront {
                     a_cur[r] = (p0 + r < L) ? 1.0f - (d + sg) : 1.0f;  // pairhmm_kernels.cuh:1336
                 }
             }
+            float qp = q_prev;
 #pragma unroll
             for (int q = 0; q < Q; ++q) {
                 uint4 w = make_uint4(0u, 0u, 0u, 0u);
@@ -135,9 +158,11 @@ struct Fp32Wavefront {
                     for (int h = 0; h < 5; ++h)
                         lam[h][s] = in ? an * ((x == 4u || h == 4 || x == (uint32_t)h) ? lm : lx) : 0.0f;
                     if (in && !(fabsf(a_cur[r]) >= kMinAlpha)) degenerate = true;
-                    dlt[r] = in ? (kBeta * d) / a_cur[r] : (c == L ? kBeta : 0.0f);
-                    sig[r] = (kBeta * sg) / an;
-                    eps[r] = in ? kEps : 1.0f;
+                    const float qc = in ? (kBeta * d) / a_cur[r] : kBeta;  // I scale of c
+                    dpv[r] = qp;
+                    ee[r] = ((in ? kEps : 1.0f) * qp) / qc;
+                    rr[r] = in ? ((kBeta * sg) / an) / qc : 0.0f;
+                    qp = qc;
                     N[r] = 0.0f;
                     D[r] = 0.0f;
                 }
@@ -145,6 +170,7 @@ struct Fp32Wavefront {
                 for (int h = 0; h < 5; ++h)
                     wtab[(h * Q + q) * 32 + lane] = make_float4(lam[h][0], lam[h][1], lam[h][2], lam[h][3]);
             }
+            const float q_last = qp;  // I scale of this lane's last position
 
             // ---------------- steps of this tile ----------------
             int t_res = 0, r_res = 0;
@@ -157,12 +183,17 @@ struct Fp32Wavefront {
             const int kg = last ? (Hc + t_res) : (Hc + G - 1);
             const bool res_lane = tile_live && last && t == t_res;
             const bool addM = r_res == R - 1;
+            // weight of the lane's last I^ in the result: beta in the carry, q when
+            // the read ends on the lane's last position
+            const float qres = addM ? q_last : kBeta;
             if (res_lane) rlane = t;
             const int kmax = (int)__reduce_max_sync(kFullMask, (unsigned)(tile_live ? kg : 0));
             const int K = (kmax + 1 + 3) & ~3;
 
-            float Ml = 0.f, Dl = 0.f, Mul = 0.f, Dul = 0.f, Iul = 0.f;
-            if (t == 0 && tile == 0) { Dl = Dbound; Dul = Dbound; }
+            // left-boundary inputs of the next step: N(j-1), I^(j), X^(j) of the
+            // column before this lane (read column -1: X = Dt = Dbound)
+            float Ml = 0.f, Mul = 0.f, Iul = 0.f, Xul = 0.f;
+            if (t == 0 && tile == 0) Xul = Dbound;
             int h = 4;
 
             // border in/out (MT only)
@@ -195,7 +226,7 @@ struct Fp32Wavefront {
                     if (t == 0) hn = (int)((wcur >> (8 * s)) & 0xffu);
                     h = hn;
                     const float4* trow = wtab + h * (Q * 32) + lane;
-                    float Ndiag = Mul, Idiag = Iul, Xdiag = Iul + Dul;
+                    float Ndiag = Mul, Idiag = Iul, Xdiag = Xul;
 #pragma unroll
                     for (int q = 0; q < Q; ++q) {
                         const float4 lam = trow[q * 32];
@@ -205,33 +236,33 @@ struct Fp32Wavefront {
                             const int r = 4 * q + u;
                             const float Nold = N[r];
                             const float Dold = D[r];
-                            N[r] = ls[u] * (Ndiag + Xdiag);
-                            D[r] = fmaf(sig[r], Nold, kEps * Dold);
-                            // eps*I carries the serial chain: one FFMA per position
-                            const float In = fmaf(eps[r], Idiag, dlt[r] * Ndiag);
+                            N[r] = ls[u] * fmaf(dpv[r], Xdiag, Ndiag);
+                            D[r] = fmaf(kEps, Dold, Nold);
+                            // e*I^ carries the serial chain: one FFMA per position
+                            const float In = fmaf(ee[r], Idiag, Ndiag);
+                            Xdiag = fmaf(rr[r], Dold, In);
                             Ndiag = Nold;
                             Idiag = In;
-                            Xdiag = In + Dold;
                         }
                     }
-                    // result (row k - t_res): It(j-1) at the lane end, plus beta*M(j) when
+                    // result (row k - t_res): I at the lane end, plus beta*M(j) when
                     // the read ends on the lane's last register
                     if (res_lane && k <= kg) {
-                        acc += Idiag;
+                        acc = fmaf(qres, Idiag, acc);
                         if (addM && k < kg) acc = fmaf(kBeta, N[R - 1], acc);
                     }
                     if (MT && writer) {
+                        // slot s holds X^(s+1), I^(s+1), N(s)
                         const int j = k - (G - 1);
-                        if (j >= 0 && j < Hc)
-                            *reinterpret_cast<float2*>(eout + j) = make_float2(N[R - 1], D[R - 1]);
-                        if (j >= 1 && j - 1 < Hc) reinterpret_cast<float*>(eout + (j - 1))[2] = Idiag;
+                        if (j >= 0 && j < Hc) reinterpret_cast<float*>(eout + j)[2] = N[R - 1];
+                        if (j >= 1 && j - 1 < Hc)
+                            *reinterpret_cast<float2*>(eout + (j - 1)) = make_float2(Xdiag, Idiag);
                     }
                     // boundary hand-off
                     Mul = Ml;
-                    Dul = Dl;
                     Ml = __shfl_up_sync(kFullMask, N[R - 1], 1, G);
-                    Dl = __shfl_up_sync(kFullMask, D[R - 1], 1, G);
                     Iul = __shfl_up_sync(kFullMask, Idiag, 1, G);
+                    Xul = __shfl_up_sync(kFullMask, Xdiag, 1, G);
                     if (MT && tile > 0) {
                         const int src = k & (G - 1);
                         const float bx = __shfl_sync(kFullMask, bcur.x, src, G);
@@ -239,7 +270,7 @@ struct Fp32Wavefront {
                         const float bz = __shfl_sync(kFullMask, bcur.z, src, G);
                         // the border is indexed by row: it feeds the diagonal of the next
                         // step directly (lanes t > 0 get theirs through the Ml -> Mul rotation)
-                        if (t == 0) { Mul = bx; Dul = by; Iul = bz; }
+                        if (t == 0) { Xul = bx; Iul = by; Mul = bz; }
                         if (src == G - 1) {
                             bcur = bnext;
                             const int64_t idx = (int64_t)k + 1 + G + t;
@@ -247,8 +278,8 @@ struct Fp32Wavefront {
                         }
                     } else if (t == 0) {
                         Ml = 0.f;
-                        Dl = Dbound;
                         Iul = 0.f;
+                        Xul = Dbound;
                     }
                 }
                 wcur = wnext;
