@@ -2,14 +2,15 @@
 // haplotype -- (read A, hap) and (read B, hap) -- with sm_100 packed FP32
 // instructions (FFMA2 / FADD2 / FMUL2 on float2 register pairs).
 //
-// The recurrence, scaling and result carry are those of wavefront_fp32.cuh;
-// every value is a float2 (x = read A, y = read B).  Because both pairs see the
-// same haplotype letter at every step, their lambda' values can be
-// interleaved when the table is built: a 16-byte shared load returns
-// (lam'_A(c), lam'_B(c), lam'_A(c+1), lam'_B(c+1)), i.e. the operands of two
-// packed cells with no register moves.  Per cell that is 3.5 packed FP32
-// instructions (same FMA-pipe cycles as 7 scalar ones, half the issue
-// slots), 1/4 shared load, and 7 shuffles per step for two pairs.
+// The recurrence, scaling and result carry are those of wavefront_fp32.cuh
+// (I, D and the diagonal sum kept divided by their input weights: four FFMA
+// and one FMUL per cell); every value is a float2 (x = read A, y = read B).
+// Because both pairs see the same haplotype letter at every step, their
+// lambda' values can be interleaved when the table is built: a 16-byte shared
+// load returns (lam'_A(c), lam'_B(c), lam'_A(c+1), lam'_B(c+1)), i.e. the
+// operands of two packed cells with no register moves.  Per cell that is 2.5
+// packed FP32 instructions (the FMA-pipe cycles of 5 scalar ones, half the
+// issue slots), 1/4 shared load, and 7 shuffles per step for two pairs.
 // Single tile only (read length <= G*R); longer reads use the scalar kernel.
 #pragma once
 
@@ -48,10 +49,21 @@ struct Fp32x2Wavefront {
         }
     }
 
+    // I scale of the position before the lane's first (1 at the read's column -1)
+    __device__ __forceinline__ static float scale_before(const uint32_t* rpack, int L, int p0, const float* ph) {
+        if (p0 == 0) return 1.0f;
+        if (p0 - 1 >= L) return kBeta;
+        const uint32_t wp = __ldg(rpack + p0 - 1);
+        const float dp = ph[(wp >> 16) & 0x7fu];
+        return (kBeta * dp) / (1.0f - (dp + ph[(wp >> 24) & 0x7fu]));
+    }
+
     // one read position of one side: lambda' for the 5 haplotype codes and the
-    // (delta', sigma', eps) coefficients (see wavefront_fp32.cuh)
+    // (q_{c-1}, e, r) coefficients (see wavefront_fp32.cuh); qp carries the I
+    // scale from one position to the next
     __device__ __forceinline__ static void position(uint32_t w, int L, int c, float ac, float an, const float* ph,
-                                                    float (&lam)[5], float& dv, float& sv, float& ev, bool& deg) {
+                                                    float (&lam)[5], float& dv, float& ev, float& rv, float& qp,
+                                                    bool& deg) {
         const uint32_t x = w & 0xffu;
         const float p = ph[(w >> 8) & 0x7fu];
         const float d = ph[(w >> 16) & 0x7fu];
@@ -62,9 +74,11 @@ struct Fp32x2Wavefront {
 #pragma unroll
         for (int h = 0; h < 5; ++h) lam[h] = in ? an * ((x == 4u || h == 4 || x == (uint32_t)h) ? lm : lx) : 0.0f;
         if (in && !(fabsf(ac) >= kMinAlpha)) deg = true;
-        dv = in ? (kBeta * d) / ac : (c == L ? kBeta : 0.0f);
-        sv = (kBeta * sgm) / an;
-        ev = in ? kEps : 1.0f;
+        const float qc = in ? (kBeta * d) / ac : kBeta;
+        dv = qp;
+        ev = ((in ? kEps : 1.0f) * qp) / qc;
+        rv = in ? ((kBeta * sgm) / an) / qc : 0.0f;
+        qp = qc;
     }
 
     __device__ static void run(const DevView& v, const Item* items, int nitem, float4* wtab, const float* ph) {
@@ -92,7 +106,8 @@ struct Fp32x2Wavefront {
         params(v, rpA, LAc, p0, ph, aA, anA);
         params(v, rpB, LBc, p0, ph, aB, anB);
         bool degA = false, degB = false;
-        float2 dl[R], sg[R], ep[R], N[R], D[R];
+        float2 dpv[R], ee[R], rr[R], N[R], D[R];
+        float qpA = scale_before(rpA, LAc, p0, ph), qpB = scale_before(rpB, LBc, p0, ph);
 #pragma unroll
         for (int q = 0; q < R / 4; ++q) {
             uint4 wa = make_uint4(0u, 0u, 0u, 0u), wb = wa;
@@ -108,8 +123,8 @@ struct Fp32x2Wavefront {
                 const float anA_r = (r + 1 < R) ? aA[r + 1 < R ? r + 1 : r] : anA;
                 const float anB_r = (r + 1 < R) ? aB[r + 1 < R ? r + 1 : r] : anB;
                 float la[5], lb[5];
-                position(was[s], LA, c, aA[r], anA_r, ph, la, dl[r].x, sg[r].x, ep[r].x, degA);
-                position(wbs[s], LB, c, aB[r], anB_r, ph, lb, dl[r].y, sg[r].y, ep[r].y, degB);
+                position(was[s], LA, c, aA[r], anA_r, ph, la, dpv[r].x, ee[r].x, rr[r].x, qpA, degA);
+                position(wbs[s], LB, c, aB[r], anB_r, ph, lb, dpv[r].y, ee[r].y, rr[r].y, qpB, degB);
 #pragma unroll
                 for (int hh = 0; hh < 5; ++hh) {
                     lamA[hh][s] = la[hh];
@@ -132,12 +147,15 @@ struct Fp32x2Wavefront {
         const int kgA = Hc + trA, kgB = Hc + trB;
         const bool resA = validA && t == trA, resB = validB && t == trB;
         const bool addMA = rrA == R - 1, addMB = rrB == R - 1;
+        // weight of the lane's last I^ in the result: beta in the carry, q when the
+        // read ends on the lane's last position
+        const float qresA = addMA ? qpA : kBeta, qresB = addMB ? qpB : kBeta;
         const int kmax = (int)__reduce_max_sync(kFullMask, (unsigned)(validA ? (kgA > kgB ? kgA : kgB) : 0));
         const int K = (kmax + 1 + 3) & ~3;
 
         const float2 k01 = f2(kEps, kEps);
-        float2 Ml = f2(0.f, 0.f), Dl = Ml, Mul = Ml, Dul = Ml, Iul = Ml;
-        if (t == 0) { Dl = f2(Dbound, Dbound); Dul = Dl; }
+        float2 Ml = f2(0.f, 0.f), Mul = Ml, Iul = Ml, Xul = Ml;
+        if (t == 0) Xul = f2(Dbound, Dbound);
         float accA = 0.f, accB = 0.f;
         int h = 4;
 
@@ -153,7 +171,7 @@ struct Fp32x2Wavefront {
                 if (t == 0) hn = (int)((wcur >> (8 * s)) & 0xffu);
                 h = hn;
                 const float4* trow = wtab + h * (Q * 32) + lane;
-                float2 Nd = Mul, Id = Iul, Xd = __fadd2_rn(Iul, Dul);
+                float2 Nd = Mul, Id = Iul, Xd = Xul;
 #pragma unroll
                 for (int qq = 0; qq < Q; ++qq) {
                     const float4 lam = trow[qq * 32];
@@ -163,31 +181,30 @@ struct Fp32x2Wavefront {
                         const float2 l2 = u ? f2(lam.z, lam.w) : f2(lam.x, lam.y);
                         const float2 No = N[r];
                         const float2 Do = D[r];
-                        N[r] = __fmul2_rn(l2, __fadd2_rn(Nd, Xd));
-                        D[r] = __ffma2_rn(sg[r], No, __fmul2_rn(k01, Do));
-                        const float2 In = __ffma2_rn(ep[r], Id, __fmul2_rn(dl[r], Nd));
+                        N[r] = __fmul2_rn(l2, __ffma2_rn(dpv[r], Xd, Nd));
+                        D[r] = __ffma2_rn(k01, Do, No);
+                        const float2 In = __ffma2_rn(ee[r], Id, Nd);
+                        Xd = __ffma2_rn(rr[r], Do, In);
                         Nd = No;
                         Id = In;
-                        Xd = __fadd2_rn(In, Do);
                     }
                 }
                 if (resA && k <= kgA) {
-                    accA += Id.x;
+                    accA = fmaf(qresA, Id.x, accA);
                     if (addMA && k < kgA) accA = fmaf(kBeta, N[R - 1].x, accA);
                 }
                 if (resB && k <= kgB) {
-                    accB += Id.y;
+                    accB = fmaf(qresB, Id.y, accB);
                     if (addMB && k < kgB) accB = fmaf(kBeta, N[R - 1].y, accB);
                 }
                 Mul = Ml;
-                Dul = Dl;
                 Ml = f2(__shfl_up_sync(kFullMask, N[R - 1].x, 1, G), __shfl_up_sync(kFullMask, N[R - 1].y, 1, G));
-                Dl = f2(__shfl_up_sync(kFullMask, D[R - 1].x, 1, G), __shfl_up_sync(kFullMask, D[R - 1].y, 1, G));
                 Iul = f2(__shfl_up_sync(kFullMask, Id.x, 1, G), __shfl_up_sync(kFullMask, Id.y, 1, G));
+                Xul = f2(__shfl_up_sync(kFullMask, Xd.x, 1, G), __shfl_up_sync(kFullMask, Xd.y, 1, G));
                 if (t == 0) {
                     Ml = f2(0.f, 0.f);
-                    Dl = f2(Dbound, Dbound);
                     Iul = f2(0.f, 0.f);
+                    Xul = f2(Dbound, Dbound);
                 }
             }
             wcur = wnext;
