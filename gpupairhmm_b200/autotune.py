@@ -78,7 +78,7 @@ def time_config(engine: Engine, batch: Batch, G: int, R: int, kind: int, repeats
     return best
 
 
-def tune(pairs_per_class: int = 6000, repeats: int = 3, device: int = 0):
+def tune(pairs_per_class: int = 60000, repeats: int = 3, device: int = 0):
     eng = Engine(device=device, fp64_rescue=False)
     eng.set_tile_table([(1 << 30, 32, 32, 1)])
     results = []
@@ -132,7 +132,8 @@ def write_outputs(results, rules):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--pairs-per-class", type=int, default=6000)
+    ap.add_argument("--pairs-per-class", type=int, default=60000,
+                    help="pairs per length class: enough that a launch is not dominated by its tail")
     ap.add_argument("--repeats", type=int, default=3)
     ap.add_argument("--device", type=int, default=0)
     ap.add_argument("--outdir", default=None, help="also copy the outputs here")
