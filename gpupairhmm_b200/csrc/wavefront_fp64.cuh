@@ -16,11 +16,18 @@
 // Values more than 2^1022 below the largest value of their lane are dropped;
 // their contribution to the result is below that factor too.
 //
-// The read-end carry runs with the in-read eps: at position L the I update
-// takes delta = eps*beta, so I there is eps times the carried value, and every
-// position beyond L multiplies by eps once more.  The result lane removes the
-// n = (positions from L to its last register) factors of eps exactly in log
-// space.  One eps for every position keeps no per-position eps registers.
+// The recurrence runs in the rescaled variables of the FP32 kernel: I and D
+// divided by the weight of the term that feeds them (q_c = beta*delta_c, or
+// beta from the read end on; s_c = beta*sigma_c), and the diagonal sum
+// X = I + D(j-1) divided by q_c, with q_{c-1} folded into the lambda table
+// and alpha_c/q_{c-1} kept per position:
+//     D^(j,c) = eps*D^(j-1,c) + M(j-1,c)
+//     I^(j,c) = e_c*I^(j,c-1) + M(j-1,c-1),        e_c = eps_c*q_{c-1}/q_c
+//     X^(j,c) = (s_c/q_c)*D^(j-1,c) + I^(j,c)
+//     M(j,c)  = lambda*q_{c-1} * ((alpha_c/q_{c-1})*M(j-1,c-1) + X^(j,c-1))
+// Five double operations per cell (four DFMA, one DMUL).  Nothing divides by
+// alpha, so pairs with alpha near or at zero are exact here.  The read-end
+// carry is that of the FP32 kernel (eps = 1 and scale beta from the read end).
 //
 // The recurrence is the plain one (alpha kept, not divided out), so pairs
 // with alpha ~ 0 are exact here.  Work split as in the FP32 kernel: groups of
@@ -35,9 +42,9 @@
 namespace phmm {
 
 struct Border64 {
-    double m, d, i;
-    int e;   // exponent of m and d (row j)
-    int ei;  // exponent of i (row j)
+    double m, x, i;
+    int e;   // exponent of m (row s)
+    int ei;  // exponent of x and i (row s + 1)
 };
 static_assert(sizeof(Border64) == 32, "Border64 is 32 bytes");
 
@@ -81,12 +88,17 @@ struct Fp64Wavefront {
         double acc = 0.0;
         int e = 0;
         int rlane = -1;
-        int ncarry = 0;  // factors of eps on the result lane's carry
 
         for (int tile = 0; tile < ntiles; ++tile) {
             const bool last = tile == ntiles - 1;
             const int p0 = tile * T + t * R;
-            double alpha[R], dlt[R], sig[R], M[R], D[R];
+            // I scale of the position before this lane's first (1 at the read's column -1)
+            double qp = 1.0;
+            if (p0 > 0) {
+                qp = beta;
+                if (p0 - 1 < L) qp = beta * (double)ph[(__ldg(rpack + p0 - 1) >> 16) & 0x7fu];
+            }
+            double aq[R], ee[R], rr[R], M[R], D[R];
 #pragma unroll
             for (int q = 0; q < Q; ++q) {
                 double lam[5][2];
@@ -100,14 +112,16 @@ struct Fp64Wavefront {
                     const float p = ph[(w >> 8) & 0x7fu];
                     const float d = ph[(w >> 16) & 0x7fu];
                     const float sg = ph[(w >> 24) & 0x7fu];
-                    const double lm = (double)(1.0f - p);
-                    const double lx = (double)(p / 3.0f);
+                    const double lm = (double)(1.0f - p) * qp;
+                    const double lx = (double)(p / 3.0f) * qp;
 #pragma unroll
                     for (int h = 0; h < 5; ++h)
                         lam[h][s] = in ? ((x == 4u || h == 4 || x == (uint32_t)h) ? lm : lx) : 0.0;
-                    alpha[r] = (double)(1.0f - (d + sg));
-                    dlt[r] = in ? beta * (double)d : (c == L ? epsd * beta : 0.0);
-                    sig[r] = beta * (double)sg;
+                    const double qc = in ? beta * (double)d : beta;
+                    aq[r] = (double)(1.0f - (d + sg)) / qp;
+                    ee[r] = ((in ? epsd : 1.0) * qp) / qc;
+                    rr[r] = in ? (beta * (double)sg) / qc : 0.0;
+                    qp = qc;
                     M[r] = 0.0;
                     D[r] = 0.0;
                 }
@@ -124,16 +138,18 @@ struct Fp64Wavefront {
             const int kg = last ? Hc + t_res : Hc + G - 1;
             const bool res_lane = valid && last && t == t_res;
             const bool addM = r_res == R - 1;
-            if (res_lane) {
-                rlane = t;
-                ncarry = addM ? 0 : R - 1 - r_res;
-            }
+            // weight of the lane's last I^ in the result: beta in the carry, q when
+            // the read ends on the lane's last position
+            const double qres = addM ? qp : beta;
+            if (res_lane) rlane = t;
             const int kmax = (int)__reduce_max_sync(kFullMask, (unsigned)(valid ? kg : 0));
             const int K = (kmax + 1 + 3) & ~3;
 
-            double Ml = 0.0, Dl = 0.0, Mul = 0.0, Dul = 0.0, Iul = 0.0;
+            // left-boundary inputs: M(j-1) with exponent eMul, I^(j) and X^(j) with eIul
+            // (read column -1: X = D = Dbound)
+            double Ml = 0.0, Mul = 0.0, Iul = 0.0, Xul = 0.0;
             int eMl = 0, eMul = 0, eIul = 0;
-            if (t == 0 && tile == 0) { Dl = Dbound; Dul = Dbound; }
+            if (t == 0 && tile == 0) Xul = Dbound;
             bool empty = !(t == 0 && tile == 0);
             const Border64* ein = scratch + ((tile - 1) & 1) * rows;
             Border64* eout = scratch + (tile & 1) * rows;
@@ -162,10 +178,10 @@ struct Fp64Wavefront {
                     if (t == 0) hn = (int)((wcur >> (8 * s)) & 0xffu);
                     h = hn;
                     // lanes fill during the first pass of the wavefront (k < G + 8)
-                    if (k0 < G + 8 && empty && (Mul != 0.0 || Dul != 0.0 || Iul != 0.0)) {
+                    if (k0 < G + 8 && empty && (Mul != 0.0 || Xul != 0.0 || Iul != 0.0)) {
                         // centre this lane's scale on the first values it receives
-                        const double md = fmax(fabs(Mul), fabs(Dul));
-                        e = md != 0.0 ? eMul - ilogb(md) : eIul - ilogb(fabs(Iul));
+                        const double xi = fmax(fabs(Xul), fabs(Iul));
+                        e = Mul != 0.0 ? eMul - ilogb(fabs(Mul)) : eIul - ilogb(xi);
                         empty = false;
                     }
                     const double2* trow = wtab + h * (Q * 32) + lane;
@@ -173,7 +189,7 @@ struct Fp64Wavefront {
                     const double fI = pow2i(e - eIul);
                     double Mdiag = Mul * fM;
                     double Idiag = Iul * fI;
-                    double Xdiag = fma(Dul, fM, Idiag);
+                    double Xdiag = Xul * fI;
 #pragma unroll
                     for (int q = 0; q < Q; ++q) {
                         const double2 lam = trow[q * 32];
@@ -183,28 +199,29 @@ struct Fp64Wavefront {
                             const int r = 2 * q + u;
                             const double Mold = M[r];
                             const double Dold = D[r];
-                            M[r] = ls[u] * fma(alpha[r], Mdiag, Xdiag);
-                            D[r] = fma(sig[r], Mold, epsd * Dold);
-                            const double In = fma(epsd, Idiag, dlt[r] * Mdiag);
+                            M[r] = ls[u] * fma(aq[r], Mdiag, Xdiag);
+                            D[r] = fma(epsd, Dold, Mold);
+                            const double In = fma(ee[r], Idiag, Mdiag);
+                            Xdiag = fma(rr[r], Dold, In);
                             Mdiag = Mold;
                             Idiag = In;
-                            Xdiag = In + Dold;
                         }
                     }
                     if (res_lane && k <= kg) {
-                        acc += Idiag;
+                        acc = fma(qres, Idiag, acc);
                         if (addM && k < kg) acc = fma(beta, M[R - 1], acc);
                     }
                     if (writer) {
+                        // slot s holds M(s), and X^(s+1), I^(s+1)
                         const int j = k - (G - 1);
-                        if (j >= 0 && j < Hc) { eout[j].m = M[R - 1]; eout[j].d = D[R - 1]; eout[j].e = e; }
-                        if (j >= 1 && j - 1 < Hc) { eout[j - 1].i = Idiag; eout[j - 1].ei = e; }
+                        if (j >= 0 && j < Hc) { eout[j].m = M[R - 1]; eout[j].e = e; }
+                        if (j >= 1 && j - 1 < Hc) { eout[j - 1].x = Xdiag; eout[j - 1].i = Idiag; eout[j - 1].ei = e; }
                     }
                     // hand-off: values travel with the sender's exponent
-                    Mul = Ml; Dul = Dl; eMul = eMl;
+                    Mul = Ml; eMul = eMl;
                     Ml = __shfl_up_sync(kFullMask, M[R - 1], 1, G);
-                    Dl = __shfl_up_sync(kFullMask, D[R - 1], 1, G);
                     Iul = __shfl_up_sync(kFullMask, Idiag, 1, G);
+                    Xul = __shfl_up_sync(kFullMask, Xdiag, 1, G);
                     const int es = __shfl_up_sync(kFullMask, e, 1, G);
                     eMl = es;
                     eIul = es;
@@ -213,12 +230,12 @@ struct Fp64Wavefront {
                             // the border is indexed by row: it feeds the next step's diagonal
                             if (k < Hc) {
                                 const Border64 b = ring[k & (kRing - 1)];
-                                Mul = b.m; Dul = b.d; eMul = b.e; Iul = b.i; eIul = b.ei;
+                                Mul = b.m; eMul = b.e; Xul = b.x; Iul = b.i; eIul = b.ei;
                             } else {
-                                Mul = 0.0; Dul = 0.0; Iul = 0.0; eMul = 0; eIul = 0;
+                                Mul = 0.0; Xul = 0.0; Iul = 0.0; eMul = 0; eIul = 0;
                             }
                         } else {
-                            Ml = 0.0; Dl = Dbound; Iul = 0.0; eMl = 0; eIul = 0;
+                            Ml = 0.0; Iul = 0.0; Xul = Dbound; eMl = 0; eIul = 0;
                         }
                     }
                     // renormalise every 16 steps (exact powers of two); a value moves by at
@@ -249,7 +266,7 @@ struct Fp64Wavefront {
             double res = -INFINITY;
             if (acc > 0.0)
                 res = log10(acc) - (double)e * 0.30102999566398119521 - log10((double)kScale) -
-                      log10((double)kBeta) - (double)ncarry * log10(epsd);
+                      log10((double)kBeta);
             v.scores[task.out] = (float)res;
         }
     }
