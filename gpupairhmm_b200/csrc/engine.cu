@@ -15,6 +15,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstring>
+#include <memory>
 #include <thread>
 
 #include "engine.hpp"
@@ -110,6 +111,8 @@ Engine::~Engine() {
         if (side_[i]) cudaStreamDestroy(side_[i]);
     }
     if (fork_) cudaEventDestroy(fork_);
+    if (span0_) cudaEventDestroy(span0_);
+    if (span1_) cudaEventDestroy(span1_);
     if (stream_) cudaStreamDestroy(stream_);
 }
 
@@ -183,6 +186,10 @@ pairhmm_status_t Engine::init() {
 }
 
 pairhmm_status_t Engine::set_tile_table(const std::vector<TileRule>& rules) {
+    if (twin_) {
+        const pairhmm_status_t t = twin_->set_tile_table(rules);
+        if (t != PAIRHMM_OK) return fail(t, twin_->last_error());
+    }
     if (rules.empty() || (int)rules.size() > kMaxBuckets) return fail(PAIRHMM_ERR_INVALID_ARGUMENT, "tile table size");
     for (size_t i = 0; i < rules.size(); ++i) {
         if (rules[i].packed && rules[i].multi_tile)
@@ -752,8 +759,8 @@ pairhmm_status_t Engine::run_pipeline(const pairhmm_batch_t& in, const BatchInde
     return PAIRHMM_OK;
 }
 
-pairhmm_status_t Engine::compute_host(const pairhmm_batch_t& b, float* scores) {
-    const auto t0 = std::chrono::steady_clock::now();
+pairhmm_status_t Engine::host_begin(const pairhmm_batch_t& b, float* scores, cudaEvent_t mark_start,
+                                    cudaEvent_t mark_end) {
     PHMM_CUDA(cudaSetDevice(opts_.device));
     // first a cheap validating pass for sizes and byte ranges, so the input
     // upload runs on helper threads while this thread builds the index
@@ -763,6 +770,7 @@ pairhmm_status_t Engine::compute_host(const pairhmm_batch_t& b, float* scores) {
     if (st != PAIRHMM_OK) return fail(st, err);
     if (rg.num_pairs > 0 && !scores) return fail(PAIRHMM_ERR_INVALID_ARGUMENT, "null scores");
     stats_ = pairhmm_stats_t{};
+    pending_ = false;
     if (rg.num_pairs == 0) return PAIRHMM_OK;
     if ((st = ensure_inputs(rg)) != PAIRHMM_OK) return st;
     cudaStream_t s = stream_;
@@ -810,16 +818,35 @@ pairhmm_status_t Engine::compute_host(const pairhmm_batch_t& b, float* scores) {
     dev.hap_lengths = in_hap_len_.as<int32_t>();
 
     PHMM_CUDA(cudaEventRecord(ev0_, s));
+    if (mark_start) PHMM_CUDA(cudaEventRecord(mark_start, s));
     if ((st = run_pipeline(dev, x, scores_.as<float>(), s)) != PAIRHMM_OK) return st;
-    // scores go straight into a page-locked caller buffer, otherwise through the
-    // uploader's page-locked slots (a copy into pageable memory would hold the
-    // driver's pageable-copy path while it waits for this stream)
+    if (mark_end) PHMM_CUDA(cudaEventRecord(mark_end, s));
+    // rescue counts and (into page-locked memory) scores come down now; scores
+    // for pageable memory go through the uploader's slots in host_end
+    PHMM_CUDA(cudaMemcpyAsync(host_hdr_, counters_.as<unsigned long long>() + kMaxBuckets,
+                              sizeof(unsigned long long) * kFp64Classes, cudaMemcpyDeviceToHost, s));
+    pend_direct_ = HostUploader::is_page_locked(scores);
+    if (pend_direct_)
+        PHMM_CUDA(cudaMemcpyAsync(scores, scores_.ptr, 4 * (size_t)x.num_pairs, cudaMemcpyDeviceToHost, s));
+    pend_scores_ = scores;
+    pend_pairs_ = x.num_pairs;
+    stats_.h2d_bytes = 4 * rn + hn + 12 * x.num_reads + 12 * x.num_haps + index_bytes(x);
+    stats_.d2h_bytes = 4 * x.num_pairs + (int64_t)sizeof(unsigned long long) * kFp64Classes;
+    stats_.launches = launches_;
+    pending_ = true;
+    return PAIRHMM_OK;
+}
+
+pairhmm_status_t Engine::host_end() {
+    if (!pending_) return PAIRHMM_OK;
+    pending_ = false;
+    PHMM_CUDA(cudaSetDevice(opts_.device));
+    cudaStream_t s = stream_;
+    if (!pend_direct_)
+        PHMM_CUDA(uploader_.download(opts_.device, pend_scores_, scores_.ptr, 4 * (size_t)pend_pairs_, s));
+    PHMM_CUDA(cudaStreamSynchronize(s));
     unsigned long long rescued_by_class[kFp64Classes] = {};
     static_assert(sizeof(rescued_by_class) <= 64, "rescue counts fit the landing spot");
-    PHMM_CUDA(cudaMemcpyAsync(host_hdr_, counters_.as<unsigned long long>() + kMaxBuckets,
-                              sizeof(rescued_by_class), cudaMemcpyDeviceToHost, s));
-    PHMM_CUDA(uploader_.download(opts_.device, scores, scores_.ptr, 4 * (size_t)x.num_pairs, s));
-    PHMM_CUDA(cudaStreamSynchronize(s));
     std::memcpy(rescued_by_class, host_hdr_, sizeof(rescued_by_class));
     float ms = 0.f, a = 0.f, b2 = 0.f, c = 0.f;
     PHMM_CUDA(cudaEventElapsedTime(&ms, ev0_, ev1_));
@@ -830,12 +857,118 @@ pairhmm_status_t Engine::compute_host(const pairhmm_batch_t& b, float* scores) {
     stats_.prep_ms = a;
     stats_.fp32_ms = b2;
     stats_.fp64_ms = c;
-    stats_.launches = launches_;
-    stats_.h2d_bytes = 4 * rn + hn + 12 * x.num_reads + 12 * x.num_haps + index_bytes(x);
-    stats_.d2h_bytes = 4 * x.num_pairs + (int64_t)sizeof(rescued_by_class);
     stats_.rescued = 0;
     for (unsigned long long r : rescued_by_class) stats_.rescued += (int64_t)r;
-    stats_.total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    return PAIRHMM_OK;
+}
+
+pairhmm_status_t Engine::compute_host(const pairhmm_batch_t& b, float* scores) {
+    const auto t0 = std::chrono::steady_clock::now();
+    // large batches run as chunks of whole records on this engine and a twin
+    // engine in turn, so a chunk's index build and upload overlap the previous
+    // chunk's kernels
+    int64_t pairs = 0;
+    if (b.num_records > 0 && b.reads_per_record && b.haps_per_record)
+        for (int64_t g = 0; g < b.num_records; ++g)
+            pairs += (int64_t)std::max(b.reads_per_record[g], 0) * std::max(b.haps_per_record[g], 0);
+    int nchunks = opts_.pipeline_chunks > 0 ? opts_.pipeline_chunks : (int)std::min<int64_t>(4, pairs / kChunkPairs);
+    if (nchunks > b.num_records) nchunks = (int)b.num_records;
+    if (nchunks < 2 || !b.read_lengths || !b.hap_lengths || !b.read_offsets || !b.hap_offsets) {
+        pairhmm_status_t st = host_begin(b, scores, nullptr, nullptr);
+        if (st == PAIRHMM_OK) st = host_end();
+        stats_.total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+        return st;
+    }
+    if (!twin_) {
+        pairhmm_options_t o = opts_;
+        o.pipeline_chunks = 1;
+        twin_ = std::make_unique<Engine>(o);
+        pairhmm_status_t st = twin_->init();
+        if (st == PAIRHMM_OK) st = twin_->set_tile_table(rules_);
+        if (st != PAIRHMM_OK) {
+            last_error_ = "twin engine: " + twin_->last_error();
+            twin_.reset();
+            return st;
+        }
+    }
+    PHMM_CUDA(cudaSetDevice(opts_.device));
+    if (!span0_) {
+        PHMM_CUDA(cudaEventCreate(&span0_));
+        PHMM_CUDA(cudaEventCreate(&span1_));
+    }
+    // chunk boundaries: records in order, about equal pairs per chunk
+    std::vector<int64_t> bound{0};
+    {
+        int64_t acc = 0, next = 1;
+        for (int64_t g = 0; g < b.num_records && (int)bound.size() < nchunks; ++g) {
+            acc += (int64_t)std::max(b.reads_per_record[g], 0) * std::max(b.haps_per_record[g], 0);
+            if (acc * nchunks >= pairs * next && g + 1 < b.num_records) {
+                bound.push_back(g + 1);
+                ++next;
+            }
+        }
+        bound.push_back(b.num_records);
+    }
+    pairhmm_stats_t sum{};
+    Engine* eng[2] = {this, twin_.get()};
+    pairhmm_status_t st = PAIRHMM_OK;
+    int64_t read0 = 0, hap0 = 0, pair0 = 0;
+    const int n = (int)bound.size() - 1;
+    auto collect = [&](Engine* e) {
+        const pairhmm_status_t r = e->host_end();
+        if (r != PAIRHMM_OK) {
+            if (e != this) last_error_ = e->last_error();
+            return r;
+        }
+        const pairhmm_stats_t& x = e->stats_;
+        sum.pairs += x.pairs;
+        sum.cells += x.cells;
+        sum.rescued += x.rescued;
+        sum.multi_tile_pairs += x.multi_tile_pairs;
+        sum.prep_ms += x.prep_ms;
+        sum.fp32_ms += x.fp32_ms;
+        sum.fp64_ms += x.fp64_ms;
+        sum.launches += x.launches;
+        sum.h2d_bytes += x.h2d_bytes;
+        sum.d2h_bytes += x.d2h_bytes;
+        return PAIRHMM_OK;
+    };
+    for (int i = 0; i < n && st == PAIRHMM_OK; ++i) {
+        Engine* e = eng[i & 1];
+        if (i >= 2) st = collect(e);  // this engine's previous chunk
+        if (st != PAIRHMM_OK) break;
+        const int64_t g0 = bound[i], g1 = bound[i + 1];
+        int64_t reads = 0, haps = 0, cp = 0;
+        for (int64_t g = g0; g < g1; ++g) {
+            reads += std::max(b.reads_per_record[g], 0);
+            haps += std::max(b.haps_per_record[g], 0);
+            cp += (int64_t)std::max(b.reads_per_record[g], 0) * std::max(b.haps_per_record[g], 0);
+        }
+        pairhmm_batch_t v = b;
+        v.num_records = g1 - g0;
+        v.reads_per_record += g0;
+        v.haps_per_record += g0;
+        v.read_offsets += read0;
+        v.read_lengths += read0;
+        v.hap_offsets += hap0;
+        v.hap_lengths += hap0;
+        st = e->host_begin(v, scores + pair0, i == 0 ? span0_ : nullptr, i == n - 1 ? span1_ : nullptr);
+        if (st != PAIRHMM_OK && e != this) last_error_ = e->last_error();
+        read0 += reads;
+        hap0 += haps;
+        pair0 += cp;
+    }
+    // the last chunks in flight (also after an error: nothing may stay queued)
+    for (int i = std::max(0, n - 2); i < n; ++i) {
+        const pairhmm_status_t r = collect(eng[i & 1]);
+        if (st == PAIRHMM_OK) st = r;
+    }
+    if (st != PAIRHMM_OK) return st;
+    float span = 0.f;
+    PHMM_CUDA(cudaEventElapsedTime(&span, span0_, span1_));
+    sum.device_ms = span;
+    sum.total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    stats_ = sum;
     return PAIRHMM_OK;
 }
 

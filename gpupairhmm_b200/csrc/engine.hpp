@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <memory>
 #include <string>
 #include <vector>
 
@@ -90,6 +91,10 @@ public:
     static pairhmm_status_t scan_inputs(const pairhmm_batch_t& b, InputRanges& r, std::string& err);
 
 private:
+    // compute_host in two halves: everything enqueued / the wait and results
+    pairhmm_status_t host_begin(const pairhmm_batch_t& b, float* scores, cudaEvent_t mark_start,
+                                cudaEvent_t mark_end);
+    pairhmm_status_t host_end();
     pairhmm_status_t upload_rules();
     pairhmm_status_t run_pipeline(const pairhmm_batch_t& dev_in, const BatchIndex& idx, float* d_scores,
                                   cudaStream_t s);
@@ -140,6 +145,14 @@ private:
     // host-to-device uploads (caller inputs, index) and the reused index
     HostUploader uploader_;
     BatchIndex idx_;
+    // pipelined compute_host: chunks of about kChunkPairs pairs (up to four)
+    // alternate between this engine and its twin
+    static constexpr int64_t kChunkPairs = int64_t(2) << 20;
+    std::unique_ptr<Engine> twin_;
+    cudaEvent_t span0_ = nullptr, span1_ = nullptr;
+    bool pending_ = false, pend_direct_ = false;
+    float* pend_scores_ = nullptr;
+    int64_t pend_pairs_ = 0;
     // page-locked landing spot for the rescue counts
     void* host_hdr_ = nullptr;
     // device memory pool of this engine's buffers (kept, not returned to the

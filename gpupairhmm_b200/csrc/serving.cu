@@ -97,6 +97,7 @@ pairhmm_status_t ServingQueue::submit(const pairhmm_batch_t& b, uint64_t* ticket
                 o.mode = PAIRHMM_MODE_ENGINE;
                 o.fp64_rescue = 1;
                 o.use_graphs = 1;
+                o.pipeline_chunks = 1;  // merged batches stay small: one pass
                 auto e = std::make_unique<Engine>(o);
                 pairhmm_status_t is = e->init();
                 if (is == PAIRHMM_OK) is = e->set_tile_table(parent_.tile_table());

@@ -117,11 +117,12 @@ def test_fp64_rescue_of_underflowing_pairs(engine):
 
 def test_fp64_length_class_boundaries(engine):
     """Unrelated high-quality reads at every FP64 length-class edge (64, 96,
-    128, 192, 256 single tile, then multi-tile): all of them underflow FP32 and
-    are recomputed by the class's FP64 kernel."""
+    128, 160, 192, 256 single tile, then multi-tile): all of them underflow FP32
+    and are recomputed by the class's FP64 kernel."""
     rng = np.random.default_rng(22)
     recs = [_record(rng, L, 400, n_reads=2, n_haps=2, bq=(35, 42), related=False)
-            for L in [1, 63, 64, 65, 95, 96, 97, 127, 128, 129, 191, 192, 193, 255, 256, 257, 300, 511, 513]]
+            for L in [1, 63, 64, 65, 95, 96, 97, 127, 128, 129, 159, 160, 161, 191, 192, 193, 255, 256, 257,
+                      300, 511, 513]]
     b = _soa(recs)
     want = oracle.batch_log10(b)
     got = engine.compute(b)
@@ -199,6 +200,27 @@ def test_graphs_and_direct_launches_agree():
     a = g.Engine(use_graphs=True).compute(b)
     c = g.Engine(use_graphs=False).compute(b)
     np.testing.assert_array_equal(a, c)
+
+
+def test_chunked_host_call_matches_one_pass():
+    """A batch run as chunks on two alternating engines (uploads overlapping
+    the previous chunk's kernels) gives bitwise the same scores and counts."""
+    b = synth.concat([synth.config1(seed=31, regions=150), synth.config3(seed=32, regions=3),
+                      synth.config2(seed=33, regions=2)])
+    one = g.Engine(pipeline_chunks=1)
+    want = one.compute(b)
+    s1 = one.stats()
+    one.close()
+    for chunks in (2, 3, 5):
+        e = g.Engine(pipeline_chunks=chunks)
+        got = e.compute(b)
+        got2 = e.compute(b.pin())
+        s = e.stats()
+        e.close()
+        assert np.array_equal(got, want) and np.array_equal(got2, want), chunks
+        assert (s.pairs, s.cells, s.rescued, s.multi_tile_pairs) == (s1.pairs, s1.cells, s1.rescued,
+                                                                     s1.multi_tile_pairs)
+        assert s.device_ms > 0
 
 
 def test_repeat_calls_are_deterministic(engine):
