@@ -31,10 +31,13 @@ def main() -> None:
     ap.add_argument("--mode", choices=["engine", "plain"], default="engine")
     ap.add_argument("--pageable", action="store_true", help="pass pageable numpy arrays (default: page-locked)")
     ap.add_argument("--device", type=int, default=0)
+    ap.add_argument("--chunks", type=int, default=1,
+                    help="pipeline_chunks of the engine (1 = one pass, whose stage times add up; 0 = auto)")
     a = ap.parse_args()
     batch = CONFIGS[a.config](a.regions, a.seed)
     inputs = batch if a.pageable else batch.pin()
-    with Engine(device=a.device, mode=MODE_PLAIN if a.mode == "plain" else MODE_ENGINE) as e:
+    with Engine(device=a.device, mode=MODE_PLAIN if a.mode == "plain" else MODE_ENGINE,
+                pipeline_chunks=a.chunks) as e:
         for i in range(a.batches):
             e.compute(inputs)
             s = e.stats()
