@@ -208,7 +208,8 @@ def run_reference(args, cfg):
 def run_binary(args, cfg):
     """A gpuPairHMM-style binary on a record file of the workload (file parse,
     upload, compute, download; output to /dev/null as the reference skips
-    formatting for it).  GCUPS as printed by the binary."""
+    formatting for it).  GCUPS as printed by the binary.  One more run writes
+    the scores to a regular file and is timed whole (`file_to_file`)."""
     import re
     from gpupairhmm_b200 import synth, CLI_PATH
     binary = ROOT / "oracle" / "_ref" / "gpuPairHMM" if args.impl == "reference-gpu" else CLI_PATH
@@ -220,6 +221,7 @@ def run_binary(args, cfg):
     os.close(fd)
     try:
         Path(path).write_text(synth.to_text(batch))
+        in_bytes = os.path.getsize(path)
         vals = []
         for i in range(args.warmup + args.steps):
             out = subprocess.run([str(binary), "--inputfile", path, "--outputfile", "/dev/null",
@@ -228,6 +230,18 @@ def run_binary(args, cfg):
             m = re.search(r"Batch processing time: ([0-9.e+-]+)s \(([0-9.e+-]+) GCUPS\)", out)
             if i >= args.warmup:
                 vals.append((float(m.group(1)), float(m.group(2))))
+        # the whole command once more with a regular output file: process start,
+        # parse, compute and the "%.5f" text, by the wall clock around it
+        fd2, opath = tempfile.mkstemp(prefix="scores_", suffix=".txt")
+        os.close(fd2)
+        try:
+            t0 = time.perf_counter()
+            subprocess.run([str(binary), "--inputfile", path, "--outputfile", opath], capture_output=True,
+                           text=True, check=True)
+            f2f = time.perf_counter() - t0
+            out_bytes = os.path.getsize(opath)
+        finally:
+            os.unlink(opath)
     finally:
         os.unlink(path)
     # median step: a single batch per process is exposed to one-off host stalls
@@ -239,7 +253,49 @@ def run_binary(args, cfg):
                       "data": "synthetic", "config": dict(cfg, pairs=batch.num_pairs, cells=batch.cells()),
                       "timing": "the binary's own batch wall clock (upload, kernels, download; file "
                                 "parsing excluded), whole batch at once; median over the steps",
-                      "step_seconds": [round(v[0], 4) for v in vals]}), flush=True)
+                      "step_seconds": [round(v[0], 4) for v in vals],
+                      "file_to_file": {"wall_s": round(f2f, 3), "gcups": round(batch.cells() / f2f / 1e9, 3),
+                                       "input_bytes": in_bytes,
+                                       "output_bytes": out_bytes,
+                                       "command": "--inputfile records --outputfile scores (default batch sizes)"}}),
+          flush=True)
+
+
+def host_io(batch, regions=4000, reps=3):
+    """Record-format throughput of the library on this host: parse (text ->
+    SoA batch) and format (scores -> "%.5f" text) through the C ABI, on all host
+    threads, best of `reps`, on the first `regions` records of the workload."""
+    import ctypes
+    import gpupairhmm_b200 as g
+    from gpupairhmm_b200 import synth
+    sub = batch.select_records(0, min(regions, batch.num_records))
+    text = synth.to_text(sub).encode()
+    L = g.lib()
+    best_p = best_f = float("inf")
+    h = ctypes.c_void_p()
+    for _ in range(reps):
+        if h.value:
+            L.pairhmm_records_free(h)
+        t0 = time.perf_counter()
+        g._check_records(L.pairhmm_records_parse(text, len(text), ctypes.byref(h)))
+        best_p = min(best_p, time.perf_counter() - t0)
+    npairs = ctypes.c_int64()
+    view = g._Batch()
+    L.pairhmm_records_view(h, ctypes.byref(view), ctypes.byref(npairs))
+    scores = (-np.random.default_rng(5).random(npairs.value) * 300).astype(np.float32)
+    need = ctypes.c_int64()
+    L.pairhmm_records_format(h, g._ptr(scores), None, 0, ctypes.byref(need))
+    buf = ctypes.create_string_buffer(need.value + 1)
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        L.pairhmm_records_format(h, g._ptr(scores), buf, need.value + 1, ctypes.byref(need))
+        best_f = min(best_f, time.perf_counter() - t0)
+    L.pairhmm_records_free(h)
+    return {"parse_gb_per_s": round(len(text) / best_p / 1e9, 3),
+            "format_mscores_per_s": round(npairs.value / best_f / 1e6, 2),
+            "threads": os.cpu_count() or 1,
+            "sample": f"first {sub.num_records} records of the workload as record text: {len(text) / 1e6:.0f} MB, "
+                      f"{npairs.value} pairs, {need.value / 1e6:.0f} MB of output; best of {reps}"}
 
 
 def percentile(xs, q):
@@ -413,6 +469,8 @@ def run_ours(args, cfg, rank, world, local_rank):
         # periodic host stalls of several hundred ms
         if world == 1 and args.serving_seconds > 0:
             line["serving"] = run_serving(args, local_rank)
+        if world == 1:
+            line["host_io"] = host_io(batch)
         line["accuracy"] = accuracy(batch, scores, args.accuracy_pairs, rng)
         if world == 1 and not args.no_cpu_baseline:
             import oracle

@@ -116,6 +116,11 @@ _SIGNATURES = {
     "pairhmm_records_view": (ctypes.c_int, [_P, _P, _P]),
     "pairhmm_records_format": (ctypes.c_int, [_P, _P, _P, ctypes.c_int64, _P]),
     "pairhmm_records_free": (None, [_P]),
+    "pairhmm_reader_open": (ctypes.c_int, [ctypes.c_char_p, _P]),
+    "pairhmm_reader_next": (ctypes.c_int, [_P, ctypes.c_int64, _P]),
+    "pairhmm_reader_close": (None, [_P]),
+    "pairhmm_records_last_error": (ctypes.c_char_p, []),
+    "pairhmm_set_host_threads": (None, [ctypes.c_int32]),
     "pairhmm_host_register": (ctypes.c_int, [_P, ctypes.c_size_t]),
     "pairhmm_host_unregister": (ctypes.c_int, [_P]),
     "pairhmm_forward_pairs_noalloc": (ctypes.c_int, [ctypes.c_int32] + [_P] * 6 + [ctypes.c_int64, ctypes.c_int32,
@@ -385,14 +390,26 @@ def version() -> str:
     return lib().pairhmm_version().decode()
 
 
+def _check_records(status: int) -> None:
+    if status != 0:
+        raise PairHMMError(status, (lib().pairhmm_records_last_error() or b"").decode(errors="replace"))
+
+
+def set_host_threads(threads: int = 0) -> None:
+    """Host threads for record parsing and formatting (0: the default, all
+    hardware threads or PAIRHMM_HOST_THREADS)."""
+    lib().pairhmm_set_host_threads(int(threads))
+
+
 class Records:
     """Records parsed by the library's parser (file_parser_worker.cu rules)."""
 
-    def __init__(self, text: str | bytes):
-        data = text.encode() if isinstance(text, str) else bytes(text)
-        h = ctypes.c_void_p()
-        _check(lib().pairhmm_records_parse(data, len(data), ctypes.byref(h)))
-        self._h = h
+    def __init__(self, text: str | bytes | None = None, *, handle: ctypes.c_void_p | None = None):
+        if handle is None:
+            data = text.encode() if isinstance(text, str) else bytes(text)
+            handle = ctypes.c_void_p()
+            _check_records(lib().pairhmm_records_parse(data, len(data), ctypes.byref(handle)))
+        self._h = handle
         s = _Batch()
         n = ctypes.c_int64()
         _check(lib().pairhmm_records_view(self._h, ctypes.byref(s), ctypes.byref(n)))
@@ -441,6 +458,43 @@ class Records:
 
 def parse_records(text: str | bytes) -> Records:
     return Records(text)
+
+
+class RecordFileReader:
+    """A record file read batch by batch (FileParserWorker::run,
+    file_parser_worker.cu:226-262): each batch holds whole records with at
+    least ``min_pairs`` pairs (<= 0: the rest of the file)."""
+
+    def __init__(self, path: str | os.PathLike):
+        h = ctypes.c_void_p()
+        _check_records(lib().pairhmm_reader_open(os.fsencode(path), ctypes.byref(h)))
+        self._h = h
+
+    def next(self, min_pairs: int = 0) -> Records | None:
+        r = ctypes.c_void_p()
+        _check_records(lib().pairhmm_reader_next(self._h, int(min_pairs), ctypes.byref(r)))
+        return Records(handle=r) if r.value else None
+
+    def batches(self, min_pairs: int = 0):
+        while (r := self.next(min_pairs)) is not None:
+            yield r
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().pairhmm_reader_close(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def read_records_file(path: str | os.PathLike) -> Records:

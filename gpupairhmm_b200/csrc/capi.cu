@@ -11,6 +11,16 @@ struct pairhmm_records {
     phmm::HostBatch batch;
 };
 
+struct pairhmm_reader {
+    explicit pairhmm_reader(const char* path) : reader(path) {}
+    phmm::RecordReader reader;
+    bool done = false;
+};
+
+namespace {
+thread_local std::string t_records_error;
+}
+
 struct pairhmm_engine {
     std::unique_ptr<phmm::Engine> engine;
     std::unique_ptr<phmm::ServingQueue> serving;
@@ -184,19 +194,66 @@ pairhmm_status_t pairhmm_batch_counts(const pairhmm_batch_t* batch, int64_t* pai
 }
 
 pairhmm_status_t pairhmm_records_parse(const char* text, int64_t length, pairhmm_records_t** out) {
+    t_records_error.clear();
     if (!out || (!text && length > 0) || length < 0) return PAIRHMM_ERR_INVALID_ARGUMENT;
     *out = nullptr;
     try {
         auto r = std::make_unique<pairhmm_records>();
-        std::string err;
-        if (!phmm::parse_records(std::string(text ? text : "", (size_t)length), r->batch, err))
+        if (!phmm::parse_records(text, (size_t)length, r->batch, t_records_error))
             return PAIRHMM_ERR_INVALID_ARGUMENT;
         *out = r.release();
         return PAIRHMM_OK;
     } catch (...) {
+        t_records_error = "host allocation failed";
         return PAIRHMM_ERR_OUT_OF_MEMORY;
     }
 }
+
+pairhmm_status_t pairhmm_reader_open(const char* path, pairhmm_reader_t** out) {
+    t_records_error.clear();
+    if (!path || !out) return PAIRHMM_ERR_INVALID_ARGUMENT;
+    *out = nullptr;
+    try {
+        auto r = std::make_unique<pairhmm_reader>(path);
+        if (!r->reader.ok()) {
+            t_records_error = r->reader.error();
+            return PAIRHMM_ERR_INVALID_ARGUMENT;
+        }
+        *out = r.release();
+        return PAIRHMM_OK;
+    } catch (...) {
+        t_records_error = "host allocation failed";
+        return PAIRHMM_ERR_OUT_OF_MEMORY;
+    }
+}
+
+pairhmm_status_t pairhmm_reader_next(pairhmm_reader_t* rd, int64_t min_pairs, pairhmm_records_t** out) {
+    t_records_error.clear();
+    if (!rd || !out) return PAIRHMM_ERR_INVALID_ARGUMENT;
+    *out = nullptr;
+    if (rd->done) return PAIRHMM_OK;
+    try {
+        auto r = std::make_unique<pairhmm_records>();
+        bool eof = false;
+        if (!rd->reader.next(r->batch, min_pairs > 0 ? min_pairs : INT64_MAX, eof)) {
+            t_records_error = rd->reader.error();
+            rd->done = true;
+            return PAIRHMM_ERR_INVALID_ARGUMENT;
+        }
+        if (eof) rd->done = true;
+        if (r->batch.num_records() > 0) *out = r.release();
+        return PAIRHMM_OK;
+    } catch (...) {
+        t_records_error = "host allocation failed";
+        return PAIRHMM_ERR_OUT_OF_MEMORY;
+    }
+}
+
+void pairhmm_reader_close(pairhmm_reader_t* rd) { delete rd; }
+
+const char* pairhmm_records_last_error(void) { return t_records_error.c_str(); }
+
+void pairhmm_set_host_threads(int32_t threads) { phmm::set_host_threads(threads); }
 
 pairhmm_status_t pairhmm_records_view(const pairhmm_records_t* r, pairhmm_batch_t* view, int64_t* num_pairs) {
     if (!r || !view) return PAIRHMM_ERR_INVALID_ARGUMENT;

@@ -4,13 +4,14 @@
 //
 //   pairhmm_b200 --inputfile in.txt --outputfile out.txt
 //                [--fileBatchsize N] [--transferBatchsize N] [--queue_depth N]
-//                [--verbose] [--checkResults] [--mode engine|plain]
+//                [--verbose] [--checkResults] [--mode engine|plain] [--hostThreads N]
 //
 // fileBatchsize: minimum pairs per parsed batch; transferBatchsize: minimum
 // pairs per engine call inside a batch; a value <= 0 means unlimited
 // (main.cu:77-83).  Defaults follow the reference's code: 1,000,000 and
 // 10,000,000 (common.cuh:19-20).  --checkResults is accepted and, as in the
-// reference, has no effect.
+// reference, has no effect.  --hostThreads sets the threads that parse and
+// format the text (default: all hardware threads).
 #include <atomic>
 #include <chrono>
 #include <condition_variable>
@@ -191,14 +192,14 @@ void writer_thread(const Options& o, Queue<PipelineData*>* in, Queue<PipelineDat
         f = std::fopen(o.outputfile.c_str(), "wb");
         if (!f) die("could not open file " + o.outputfile);
     }
-    std::string text;
+    std::vector<std::string> parts;
     for (;;) {
         PipelineData* d = in->pop();
         if (!d) break;
         if (!no_output) {
-            text.clear();
-            phmm::format_scores(d->batch, d->scores.data(), text);
-            if (std::fwrite(text.data(), 1, text.size(), f) != text.size()) die("write failed");
+            phmm::format_scores_parts(d->batch, d->scores.data(), parts);  // on the host threads
+            for (const std::string& text : parts)
+                if (std::fwrite(text.data(), 1, text.size(), f) != text.size()) die("write failed");
         }
         d->batch.clear();
         out->push(d);
@@ -226,6 +227,7 @@ int main(int argc, char** argv) {
         else if (a == "--fileBatchsize") o.fileBatchsize = std::atoll(val("--fileBatchsize").c_str());
         else if (a == "--queue_depth") o.queue_depth = std::atoi(val("--queue_depth").c_str());
         else if (a == "--checkResults") o.checkResults = true;
+        else if (a == "--hostThreads") pairhmm_set_host_threads(std::atoi(val("--hostThreads").c_str()));
         else if (a == "--verbose") o.verbose = true;
         else if (a == "--mode") {
             const std::string m = val("--mode");

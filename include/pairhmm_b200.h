@@ -178,14 +178,24 @@ pairhmm_status_t pairhmm_probe_fp32_peak(int32_t device, int32_t milliseconds, d
 
 /*
  * Record file format (README.md:41-61).  A parsed buffer owns its arrays; the
- * view points into them (valid until pairhmm_records_free).
+ * view points into them (valid until pairhmm_records_free).  Parsing and
+ * formatting run on several host threads (pairhmm_set_host_threads); the
+ * results do not depend on the thread count.
  *   pairhmm_records_parse   FileParserWorker::parseNextSequenceGroup +
  *                           convertGroupsToBatchInplace (file_parser_worker.cu:88-218):
  *                           R/H header, 5 fields per read at k*(L+1), quality - 33,
  *                           4 - len%4 bytes of 'N' padding (quality 'N'-33)
  *   pairhmm_records_format  OutputWriterWorker::run (output_writer_worker.cu:107-135):
- *                           "%d %d\n", then R lines of H "%.5f" joined by spaces.
+ *                           "%d %d\n", then R lines of H "%.5f" joined by spaces,
+ *                           the same text as the C library's printf gives.
  *                           With buf == NULL (or capacity too small) only *len is set.
+ *   pairhmm_reader_*        FileParserWorker::run (file_parser_worker.cu:226-262): a
+ *                           record file read batch by batch; next returns whole records
+ *                           holding at least min_pairs pairs (<= 0: the rest of the
+ *                           file), or *records = NULL at the end of the file.  A regular
+ *                           file is mapped; other files are read whole at open.
+ *   pairhmm_records_last_error  why the last parse or read on this thread failed
+ *                           (names the 1-based line), "" if it did not.
  */
 typedef struct pairhmm_records pairhmm_records_t;
 pairhmm_status_t pairhmm_records_parse(const char* text, int64_t length, pairhmm_records_t** records);
@@ -194,6 +204,15 @@ pairhmm_status_t pairhmm_records_view(const pairhmm_records_t* records, pairhmm_
 pairhmm_status_t pairhmm_records_format(const pairhmm_records_t* records, const float* scores, char* buf,
                                         int64_t capacity, int64_t* length);
 void pairhmm_records_free(pairhmm_records_t* records);
+typedef struct pairhmm_reader pairhmm_reader_t;
+pairhmm_status_t pairhmm_reader_open(const char* path, pairhmm_reader_t** reader);
+pairhmm_status_t pairhmm_reader_next(pairhmm_reader_t* reader, int64_t min_pairs, pairhmm_records_t** records);
+void pairhmm_reader_close(pairhmm_reader_t* reader);
+const char* pairhmm_records_last_error(void);
+/* Host threads for record parsing and formatting: threads > 0 sets the count,
+ * 0 returns to the default (PAIRHMM_HOST_THREADS, else all hardware threads;
+ * at most 64). */
+void pairhmm_set_host_threads(int32_t threads);
 
 /*
  * No counterpart in the reference.  Allocation-free forward for callers that
