@@ -43,33 +43,13 @@ struct Options {
     std::string outputfile;
 };
 
+// One batch buffer of the ring.  Its arrays stay pageable: the engine uploads
+// them through its page-locked staging slots.  Page-locking them per batch
+// (cudaHostRegister) took about 0.7 s per GB on a B200 host and waited for the
+// CUDA context, against about 14 ms more upload time per GB when staged.
 struct PipelineData {
     phmm::HostBatch batch;
     std::vector<float> scores;
-    std::vector<void*> pinned;  // batch arrays page-locked by the parser thread
-
-    // page-lock the parsed arrays so the engine uploads them by DMA; a failed
-    // registration only means that array is staged through the engine's buffers
-    void pin() {
-        auto reg = [&](void* p, size_t n) {
-            if (n && pairhmm_host_register(p, n) == PAIRHMM_OK) pinned.push_back(p);
-        };
-        phmm::HostBatch& b = batch;
-        reg(b.read_bases.data(), b.read_bases.size());
-        reg(b.base_quals.data(), b.base_quals.size());
-        reg(b.ins_quals.data(), b.ins_quals.size());
-        reg(b.del_quals.data(), b.del_quals.size());
-        reg(b.hap_bases.data(), b.hap_bases.size());
-        reg(b.read_offsets.data(), 8 * b.read_offsets.size());
-        reg(b.read_lengths.data(), 4 * b.read_lengths.size());
-        reg(b.hap_offsets.data(), 8 * b.hap_offsets.size());
-        reg(b.hap_lengths.data(), 4 * b.hap_lengths.size());
-        reg(scores.data(), 4 * scores.size());
-    }
-    void unpin() {
-        for (void* p : pinned) pairhmm_host_unregister(p);
-        pinned.clear();
-    }
 };
 
 template <class T>
@@ -96,6 +76,16 @@ private:
 
 std::atomic<bool> g_failed{false};
 
+// host-side stage times for --verbose (seconds, summed over batches)
+struct HostTimes {
+    double parse = 0, format_write = 0, engine_start = 0;
+};
+HostTimes g_times;
+
+double since(std::chrono::steady_clock::time_point t0) {
+    return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+}
+
 void die(const std::string& msg) {
     std::cerr << msg << "\n";
     std::exit(EXIT_FAILURE);  // as the reference's workers do (gpuworker.cu:33-39)
@@ -106,12 +96,12 @@ void parser_thread(const Options& o, Queue<PipelineData*>* in, Queue<PipelineDat
     if (!reader.ok()) die(reader.error());
     for (;;) {
         PipelineData* d = in->pop();
-        d->unpin();
         d->batch.clear();
         bool eof = false;
+        auto t0 = std::chrono::steady_clock::now();
         if (!reader.next(d->batch, o.fileBatchsize, eof)) die("parse error: " + reader.error());
+        g_times.parse += since(t0);
         d->scores.resize((size_t)std::max<int64_t>(d->batch.pairs, 1));
-        d->pin();
         if (d->batch.num_records() > 0) out->push(d);
         else in->push(d);
         if (eof) break;
@@ -125,6 +115,7 @@ void gpu_thread(const Options& o, Queue<PipelineData*>* in, Queue<PipelineData*>
     pairhmm_default_options(&eo);
     eo.mode = o.mode;
     pairhmm_engine_t* eng = nullptr;
+    const auto t_engine = std::chrono::steady_clock::now();
     pairhmm_status_t st = pairhmm_engine_create(&eo, &eng);
     if (st != PAIRHMM_OK) die(std::string("engine: ") + pairhmm_status_string(st));
     {
@@ -139,11 +130,12 @@ void gpu_thread(const Options& o, Queue<PipelineData*>* in, Queue<PipelineData*>
             pairhmm_compute_host(eng, &v, &score);
         }
     }
+    g_times.engine_start = since(t_engine);
     for (;;) {
         PipelineData* d = in->pop();
         if (!d) break;
         const auto t0 = std::chrono::steady_clock::now();
-        phmm::HostBatch& b = d->batch;  // scores were sized (and page-locked) by the parser
+        phmm::HostBatch& b = d->batch;  // scores were sized by the parser
         // transfer chunks: consecutive records with at least transferBatchsize pairs
         int64_t g = 0, read0 = 0, hap0 = 0, pair0 = 0;
         const int64_t ng = b.num_records();
@@ -197,9 +189,11 @@ void writer_thread(const Options& o, Queue<PipelineData*>* in, Queue<PipelineDat
         PipelineData* d = in->pop();
         if (!d) break;
         if (!no_output) {
+            const auto t0 = std::chrono::steady_clock::now();
             phmm::format_scores_parts(d->batch, d->scores.data(), parts);  // on the host threads
             for (const std::string& text : parts)
                 if (std::fwrite(text.data(), 1, text.size(), f) != text.size()) die("write failed");
+            g_times.format_write += since(t0);
         }
         d->batch.clear();
         out->push(d);
@@ -253,14 +247,17 @@ int main(int argc, char** argv) {
     }
     double seconds = 0.0;
     int64_t cells = 0;
+    const auto t_start = std::chrono::steady_clock::now();
     std::thread tp(parser_thread, std::cref(o), &to_parser, &to_gpu);
     std::thread tg(gpu_thread, std::cref(o), &to_gpu, &to_writer, &seconds, &cells);
     std::thread tw(writer_thread, std::cref(o), &to_writer, &to_parser);
     tp.join();
     tg.join();
     tw.join();
-    for (auto& b : buffers) b->unpin();
     const double gcups = seconds > 0 ? cells / 1e9 / seconds : 0.0;
+    if (o.verbose)
+        std::cout << "Host stages: engine start-up " << g_times.engine_start << "s, parse " << g_times.parse
+                  << "s, format+write " << g_times.format_write << "s; all stages " << since(t_start) << "s\n";
     std::cout << "Batch processing time: " << seconds << "s (" << gcups << " GCUPS)\n";
     return 0;
 }
