@@ -71,7 +71,7 @@ class _Options(ctypes.Structure):
         ("use_graphs", ctypes.c_int32),
         ("device_budget_bytes", ctypes.c_int64),
         ("pipeline_chunks", ctypes.c_int32),
-        ("reserved", ctypes.c_int32),
+        ("gcp", ctypes.c_int32),
     ]
 
 
@@ -261,13 +261,17 @@ class Engine:
     """A device engine (resident tables, streams, device buffers)."""
 
     def __init__(self, device: int = 0, mode: int = MODE_ENGINE, fp64_rescue: bool = True,
-                 use_graphs: bool = True, device_budget_bytes: int = 0, pipeline_chunks: int = 0):
+                 use_graphs: bool = True, device_budget_bytes: int = 0, pipeline_chunks: int = 0,
+                 gcp: bool = False):
+        """gcp=True: eps and beta per read from its first gcp quality (the
+        reference's CPU recurrence) instead of the GPU path's 0.1 / 0.9."""
         L = lib()
         o = _Options()
         L.pairhmm_default_options(ctypes.byref(o))
         o.device, o.mode, o.fp64_rescue, o.use_graphs = device, mode, int(fp64_rescue), int(use_graphs)
         o.device_budget_bytes = device_budget_bytes
         o.pipeline_chunks = pipeline_chunks
+        o.gcp = int(gcp)
         h = ctypes.c_void_p()
         _check(L.pairhmm_engine_create(ctypes.byref(o), ctypes.byref(h)))
         self._h = h

@@ -63,7 +63,7 @@ void pairhmm_default_options(pairhmm_options_t* o) {
     o->use_graphs = 1;
     o->device_budget_bytes = 0;
     o->pipeline_chunks = 0;
-    o->reserved = 0;
+    o->gcp = 0;
 }
 
 pairhmm_status_t pairhmm_engine_create(const pairhmm_options_t* opts, pairhmm_engine_t** out) {

@@ -77,6 +77,10 @@ struct DevView {
     unsigned long long* rescue_count;  // [kFp64Classes]
     int rescue_enabled;
     const float* ph2pr;         // 128 floats in global memory
+    // gcp mode only (else null): the gcp quality of each read's first position,
+    // clamped to 127.  eps = p(gcp), beta = 1 - eps for all of the read's pairs,
+    // as the reference's CPU recurrence takes them (gpuworker.cuh:1009, 1048-1049).
+    const uint8_t* read_gcp;
 };
 
 __device__ __forceinline__ uint32_t code_of(uint8_t c) {

@@ -48,6 +48,15 @@ std::vector<TileRule> plain_rules() {
     };
 }
 
+std::vector<TileRule> gcp_rules() {
+    // gcp mode (eps and beta per read): the scalar kernels compiled with that
+    // option (fp32_gcp.cu), one per length class.
+    return {
+        {64, 4, 16, false},   {128, 8, 16, false},  {160, 8, 20, false},    {256, 16, 16, false},
+        {512, 32, 16, false}, {1024, 32, 32, false}, {1 << 30, 32, 32, true},
+    };
+}
+
 inline int64_t round_up(int64_t x, int64_t m) { return (x + m - 1) / m * m; }
 
 int bucket_of_host(int L, const std::vector<TileRule>& rules) {
@@ -83,7 +92,7 @@ void DevBuf::release() {
 }
 
 Engine::Engine(const pairhmm_options_t& opts) : opts_(opts) {
-    rules_ = opts_.mode == PAIRHMM_MODE_PLAIN ? plain_rules() : engine_default_rules();
+    rules_ = opts_.mode == PAIRHMM_MODE_PLAIN ? plain_rules() : opts_.gcp ? gcp_rules() : engine_default_rules();
 }
 
 std::vector<DevBuf*> Engine::all_buffers() {
@@ -91,7 +100,8 @@ std::vector<DevBuf*> Engine::all_buffers() {
             &in_iq_, &in_dq_, &in_read_off_, &in_read_len_, &in_hap_bases_, &in_hap_off_, &in_hap_len_,
             &read_record_, &read_local_, &rec_haps_, &rec_hap_base_, &rec_pair_base_, &read_start_,
             &hap_start_, &read_pack_, &hap_code_, &hist_, &cursor_, &items_, &rescue_, &counters_,
-            &sched_, &scores_, &scratch_, &lens_tmp_, &unit_read0_, &unit_read1_, &unit_bucket_, &rescue_off_};
+            &sched_, &scores_, &scratch_, &lens_tmp_, &unit_read0_, &unit_read1_, &unit_bucket_, &rescue_off_,
+            &in_gq_, &read_gcp_};
 }
 
 Engine::~Engine() {
@@ -137,6 +147,8 @@ pairhmm_status_t Engine::init() {
     cudaError_t e = cudaGetDeviceCount(&ndev);
     if (e != cudaSuccess || ndev == 0) return fail(PAIRHMM_ERR_UNSUPPORTED, "no CUDA device");
     if (opts_.device < 0 || opts_.device >= ndev) return fail(PAIRHMM_ERR_INVALID_ARGUMENT, "bad device ordinal");
+    if (opts_.gcp && opts_.mode == PAIRHMM_MODE_PLAIN)
+        return fail(PAIRHMM_ERR_INVALID_ARGUMENT, "gcp mode runs in the engine form, not the plain form");
     PHMM_CUDA(cudaSetDevice(opts_.device));
     cudaDeviceProp prop{};
     PHMM_CUDA(cudaGetDeviceProperties(&prop, opts_.device));
@@ -171,8 +183,9 @@ pairhmm_status_t Engine::init() {
     for (const ConfigInfo& c : fp32_configs())
         PHMM_CUDA(cudaFuncSetAttribute(c.kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c.smem_bytes));
     for (int c = 0; c < kFp64Classes; ++c)
-        PHMM_CUDA(cudaFuncSetAttribute(fp64_kernel(c), cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)fp64_smem_bytes(c)));
+        for (const bool gcp : {false, true})
+            PHMM_CUDA(cudaFuncSetAttribute(fp64_kernel(c, gcp), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)fp64_smem_bytes(c)));
 
     // probability table p(q) = float(10^(-q/10)) (gpuworker.cuh:473-486)
     float table[128];
@@ -194,7 +207,7 @@ pairhmm_status_t Engine::set_tile_table(const std::vector<TileRule>& rules) {
     for (size_t i = 0; i < rules.size(); ++i) {
         if (rules[i].packed && rules[i].multi_tile)
             return fail(PAIRHMM_ERR_INVALID_ARGUMENT, "packed rules are single tile");
-        if (!find_fp32_config(rules[i].G, rules[i].R, rules[i].multi_tile, rules[i].packed))
+        if (!find_fp32_config(rules[i].G, rules[i].R, rules[i].multi_tile, rules[i].packed, opts_.gcp != 0))
             return fail(PAIRHMM_ERR_INVALID_ARGUMENT, "tile table names a configuration that is not compiled");
         if (i > 0 && rules[i].max_len <= rules[i - 1].max_len)
             return fail(PAIRHMM_ERR_INVALID_ARGUMENT, "tile table bounds must increase");
@@ -215,7 +228,8 @@ pairhmm_status_t Engine::upload_rules() {
     rule_cfg_.assign(nb, nullptr);
     std::vector<int32_t> maxlen(nb), rank(nb), per(nb), cfg(nb);
     for (int b = 0; b < nb; ++b) {
-        rule_cfg_[b] = find_fp32_config(rules_[b].G, rules_[b].R, rules_[b].multi_tile, rules_[b].packed);
+        rule_cfg_[b] =
+            find_fp32_config(rules_[b].G, rules_[b].R, rules_[b].multi_tile, rules_[b].packed, opts_.gcp != 0);
         if (!rule_cfg_[b]) return fail(PAIRHMM_ERR_INVALID_ARGUMENT, "tile rule without compiled kernel");
         maxlen[b] = rules_[b].max_len;
         rank[b] = opts_.mode == PAIRHMM_MODE_PLAIN ? b : nb - 1 - b;
@@ -393,7 +407,7 @@ pairhmm_status_t Engine::build_index(const pairhmm_batch_t& b, const std::vector
     return PAIRHMM_OK;
 }
 
-pairhmm_status_t Engine::scan_inputs(const pairhmm_batch_t& b, InputRanges& r, std::string& err) {
+pairhmm_status_t Engine::scan_inputs(const pairhmm_batch_t& b, InputRanges& r, std::string& err, bool gcp) {
     r = InputRanges{};
     if (b.num_records < 0) { err = "num_records < 0"; return PAIRHMM_ERR_INVALID_ARGUMENT; }
     if (b.num_records == 0) return PAIRHMM_OK;
@@ -418,11 +432,19 @@ pairhmm_status_t Engine::scan_inputs(const pairhmm_batch_t& b, InputRanges& r, s
         err = "null haplotype arrays";
         return PAIRHMM_ERR_INVALID_ARGUMENT;
     }
+    if (gcp && r.num_reads > 0 && !b.gcp_quals) {
+        err = "gcp mode needs the gcp quality array";
+        return PAIRHMM_ERR_INVALID_ARGUMENT;
+    }
     for (int64_t i = 0; i < r.num_reads; ++i) {
         const int32_t L = b.read_lengths[i];
         const int64_t o = b.read_offsets[i];
         if (L < 1) { err = "read length < 1"; return PAIRHMM_ERR_INVALID_ARGUMENT; }
         if (o < 0) { err = "negative read offset"; return PAIRHMM_ERR_INVALID_ARGUMENT; }
+        if (gcp && b.gcp_quals[o] == 0) {
+            err = "gcp quality 0 (eps = 1, beta = 0) has no gap-to-match transition to rescale by";
+            return PAIRHMM_ERR_INVALID_ARGUMENT;
+        }
         r.read_min = i == 0 ? o : std::min(r.read_min, o);
         r.read_end = std::max(r.read_end, o + L);
     }
@@ -445,6 +467,7 @@ pairhmm_status_t Engine::ensure_inputs(const InputRanges& r) {
     PHMM_CUDA(in_bq_.ensure(rb));
     PHMM_CUDA(in_iq_.ensure(rb));
     PHMM_CUDA(in_dq_.ensure(rb));
+    if (opts_.gcp) PHMM_CUDA(in_gq_.ensure(rb));
     PHMM_CUDA(in_read_off_.ensure(8 * nr));
     PHMM_CUDA(in_read_len_.ensure(4 * nr));
     PHMM_CUDA(in_hap_bases_.ensure(hb));
@@ -464,6 +487,7 @@ pairhmm_status_t Engine::ensure_buffers(const BatchIndex& x, bool host_inputs) {
         PHMM_CUDA(in_bq_.ensure(rb));
         PHMM_CUDA(in_iq_.ensure(rb));
         PHMM_CUDA(in_dq_.ensure(rb));
+        if (opts_.gcp) PHMM_CUDA(in_gq_.ensure(rb));
         PHMM_CUDA(in_read_off_.ensure(8 * nr));
         PHMM_CUDA(in_read_len_.ensure(4 * nr));
         PHMM_CUDA(in_hap_bases_.ensure(hb));
@@ -473,6 +497,7 @@ pairhmm_status_t Engine::ensure_buffers(const BatchIndex& x, bool host_inputs) {
     }
     PHMM_CUDA(read_record_.ensure(4 * nr));
     PHMM_CUDA(read_local_.ensure(4 * nr));
+    if (opts_.gcp) PHMM_CUDA(read_gcp_.ensure(nr));
     PHMM_CUDA(rec_haps_.ensure(4 * ng));
     PHMM_CUDA(rec_hap_base_.ensure(8 * ng));
     PHMM_CUDA(rec_pair_base_.ensure(8 * ng));
@@ -540,6 +565,8 @@ pairhmm_status_t Engine::enqueue_pipeline(const pairhmm_batch_t& in, const Batch
     pa.hap_bases = in.hap_bases;
     pa.hap_offsets = in.hap_offsets;
     pa.hap_lengths = in.hap_lengths;
+    pa.gcp_quals = opts_.gcp ? in.gcp_quals : nullptr;
+    pa.read_gcp = opts_.gcp ? read_gcp_.as<uint8_t>() : nullptr;
     pa.read_record = read_record_.as<int32_t>();
     pa.read_local = read_local_.as<int32_t>();
     pa.rec_haps = rec_haps_.as<int32_t>();
@@ -605,6 +632,7 @@ pairhmm_status_t Engine::enqueue_pipeline(const pairhmm_batch_t& in, const Batch
     v.rescue_count = counters + kMaxBuckets;
     v.rescue_enabled = (!plain && opts_.fp64_rescue) ? 1 : 0;
     v.ph2pr = ph2pr_.as<float>();
+    v.read_gcp = pa.read_gcp;
 
     // engine form: the stage's launches go round-robin onto the side streams
     // (forked from s, joined back below); the plain form keeps one stream
@@ -642,6 +670,7 @@ pairhmm_status_t Engine::enqueue_pipeline(const pairhmm_batch_t& in, const Batch
             Fp64LaunchArgs fa{};
             fa.view = v;
             fa.cls = c;
+            fa.gcp = opts_.gcp != 0;
             fa.items = rescue_.as<Task>() + x.class_start[c];
             fa.count = counters + kMaxBuckets + c;
             fa.counter = counters + kMaxBuckets + kFp64Classes + c;
@@ -696,7 +725,7 @@ Engine::Plan Engine::make_plan(const BatchIndex& x) const {
         p.persistent[b] = (!plain || grid < need_blocks) ? 1 : 0;
     }
     for (int c = 0; c < kFp64Classes; ++c) {
-        int64_t grid = persistent_grid(fp64_kernel(c), fp64_smem_bytes(c));
+        int64_t grid = persistent_grid(fp64_kernel(c, opts_.gcp != 0), fp64_smem_bytes(c));
         const int64_t per_warp = (int64_t)fp64_scratch_bytes_per_row(c) * p.rows;
         if (per_warp > 0) {
             grid = std::min<int64_t>(grid, std::max<int64_t>(1, kScratchBudget / (per_warp * kWarpsPerBlock)));
@@ -766,7 +795,7 @@ pairhmm_status_t Engine::host_begin(const pairhmm_batch_t& b, float* scores, cud
     // upload runs on helper threads while this thread builds the index
     InputRanges rg;
     std::string err;
-    pairhmm_status_t st = scan_inputs(b, rg, err);
+    pairhmm_status_t st = scan_inputs(b, rg, err, opts_.gcp != 0);
     if (st != PAIRHMM_OK) return fail(st, err);
     if (rg.num_pairs > 0 && !scores) return fail(PAIRHMM_ERR_INVALID_ARGUMENT, "null scores");
     stats_ = pairhmm_stats_t{};
@@ -778,7 +807,7 @@ pairhmm_status_t Engine::host_begin(const pairhmm_batch_t& b, float* scores, cud
     // are shifted so the caller's absolute offsets stay valid
     const int64_t rlo = rg.read_min, rn = rg.read_end - rg.read_min;
     const int64_t hlo = rg.hap_min, hn = rg.hap_end - rg.hap_min;
-    const std::vector<HostUploader::Copy> inputs = {
+    std::vector<HostUploader::Copy> inputs = {
         {in_read_bases_.ptr, b.read_bases + rlo, (size_t)rn},
         {in_bq_.ptr, b.base_quals + rlo, (size_t)rn},
         {in_iq_.ptr, b.ins_quals + rlo, (size_t)rn},
@@ -789,6 +818,7 @@ pairhmm_status_t Engine::host_begin(const pairhmm_batch_t& b, float* scores, cud
         {in_hap_off_.ptr, b.hap_offsets, (size_t)(8 * rg.num_haps)},
         {in_hap_len_.ptr, b.hap_lengths, (size_t)(4 * rg.num_haps)},
     };
+    if (opts_.gcp) inputs.push_back({in_gq_.ptr, b.gcp_quals + rlo, (size_t)rn});
     cudaError_t up = uploader_.start(opts_.device, inputs, s);
     st = build_index(b, rules_, idx_, err);
     const cudaError_t upf = uploader_.finish();
@@ -810,7 +840,7 @@ pairhmm_status_t Engine::host_begin(const pairhmm_batch_t& b, float* scores, cud
     dev.base_quals = shifted(in_bq_, rlo);
     dev.ins_quals = shifted(in_iq_, rlo);
     dev.del_quals = shifted(in_dq_, rlo);
-    dev.gcp_quals = nullptr;
+    dev.gcp_quals = opts_.gcp ? shifted(in_gq_, rlo) : nullptr;
     dev.read_offsets = in_read_off_.as<int64_t>();
     dev.read_lengths = in_read_len_.as<int32_t>();
     dev.hap_bases = shifted(in_hap_bases_, hlo);
@@ -979,6 +1009,7 @@ pairhmm_status_t Engine::compute_device(const pairhmm_batch_t& b, int32_t, int32
     if (b.num_records < 0) return fail(PAIRHMM_ERR_INVALID_ARGUMENT, "num_records < 0");
     if (b.num_records == 0) { stats_ = pairhmm_stats_t{}; return PAIRHMM_OK; }
     if (!b.reads_per_record || !b.haps_per_record) return fail(PAIRHMM_ERR_INVALID_ARGUMENT, "null record arrays");
+    if (opts_.gcp && !b.gcp_quals) return fail(PAIRHMM_ERR_INVALID_ARGUMENT, "gcp mode needs the gcp quality array");
     // the host needs the record structure and lengths to derive the index
     std::vector<int32_t> rpr(b.num_records), hpr(b.num_records);
     PHMM_CUDA(cudaMemcpyAsync(rpr.data(), b.reads_per_record, 4 * b.num_records, cudaMemcpyDeviceToHost, stream));

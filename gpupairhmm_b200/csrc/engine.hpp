@@ -83,12 +83,14 @@ public:
     pairhmm_status_t set_tile_table(const std::vector<TileRule>& rules);
     const std::vector<TileRule>& tile_table() const { return rules_; }
     int device() const { return opts_.device; }
+    bool gcp() const { return opts_.gcp != 0; }
     int64_t budget_bytes() const { return opts_.device_budget_bytes; }
     int num_sms() const { return num_sms_; }
 
     static pairhmm_status_t build_index(const pairhmm_batch_t& b, const std::vector<TileRule>& rules,
                                         BatchIndex& idx, std::string& err);
-    static pairhmm_status_t scan_inputs(const pairhmm_batch_t& b, InputRanges& r, std::string& err);
+    // gcp: the batch must carry gcp qualities, none 0 at a read's first position
+    static pairhmm_status_t scan_inputs(const pairhmm_batch_t& b, InputRanges& r, std::string& err, bool gcp);
 
 private:
     // compute_host in two halves: everything enqueued / the wait and results
@@ -137,6 +139,7 @@ private:
     // device buffers
     DevBuf ph2pr_, rules_maxlen_, rules_rank_, per_task_, config_;
     DevBuf in_read_bases_, in_bq_, in_iq_, in_dq_, in_read_off_, in_read_len_;
+    DevBuf in_gq_, read_gcp_;  // gcp mode: uploaded gcp qualities, per-read gcp
     DevBuf in_hap_bases_, in_hap_off_, in_hap_len_;
     DevBuf read_record_, read_local_, rec_haps_, rec_hap_base_, rec_pair_base_, read_start_, hap_start_;
     DevBuf unit_read0_, unit_read1_, unit_bucket_;

@@ -31,6 +31,7 @@ struct Fp32LaunchArgs {
 struct Fp64LaunchArgs {
     DevView view;
     int cls;                         // length class (fp64_class)
+    bool gcp;                        // gcp mode kernel
     const Task* items;               // that class's rescue list
     const unsigned long long* count; // number of items (device)
     unsigned long long* counter;     // task counter
@@ -45,6 +46,7 @@ struct ConfigInfo {
     int R;
     bool multi_tile;
     bool packed;                     // two reads per group with packed FP32 (single tile)
+    bool gcp;                        // eps/beta per read (gcp mode)
     int tile() const { return G * R; }
     int per_warp() const { return 32 / G; }   // items per warp task
     size_t smem_bytes;               // dynamic shared memory per CTA
@@ -55,14 +57,15 @@ struct ConfigInfo {
 
 // All compiled FP32 configurations.
 const std::vector<ConfigInfo>& fp32_configs();
-const ConfigInfo* find_fp32_config(int G, int R, bool multi_tile, bool packed = false);
+const ConfigInfo* find_fp32_config(int G, int R, bool multi_tile, bool packed = false, bool gcp = false);
 
 // FP64 pass, one kernel per length class: (G, R) = (8, 8), (16, 8) single
 // tile and (32, 8) multi-tile.
+// gcp selects the gcp-mode kernels (eps/beta per read).
 cudaError_t launch_fp64_rescue(const Fp64LaunchArgs& a);
 size_t fp64_smem_bytes(int cls);
 size_t fp64_scratch_bytes_per_row(int cls);  // per warp, per border row
-const void* fp64_kernel(int cls);
+const void* fp64_kernel(int cls, bool gcp = false);
 int fp64_per_warp(int cls);
 
 // Preparation kernels.

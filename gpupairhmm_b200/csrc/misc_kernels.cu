@@ -14,6 +14,7 @@ void register_fp32_g4(std::vector<ConfigInfo>& out);
 void register_fp32_g8(std::vector<ConfigInfo>& out);
 void register_fp32_g16(std::vector<ConfigInfo>& out);
 void register_fp32_g32(std::vector<ConfigInfo>& out);
+void register_fp32_gcp(std::vector<ConfigInfo>& out);
 
 const std::vector<ConfigInfo>& fp32_configs() {
     static std::vector<ConfigInfo> all;
@@ -23,13 +24,14 @@ const std::vector<ConfigInfo>& fp32_configs() {
         register_fp32_g8(all);
         register_fp32_g16(all);
         register_fp32_g32(all);
+        register_fp32_gcp(all);
     });
     return all;
 }
 
-const ConfigInfo* find_fp32_config(int G, int R, bool multi_tile, bool packed) {
+const ConfigInfo* find_fp32_config(int G, int R, bool multi_tile, bool packed, bool gcp) {
     for (const auto& c : fp32_configs())
-        if (c.G == G && c.R == R && c.multi_tile == multi_tile && c.packed == packed) return &c;
+        if (c.G == G && c.R == R && c.multi_tile == multi_tile && c.packed == packed && c.gcp == gcp) return &c;
     return nullptr;
 }
 
@@ -79,6 +81,14 @@ size_t fp64_smem_for() {
            (size_t)kWarpsPerBlock * W::kRing * sizeof(Border64);
 }
 
+// gcp-mode twins of the class kernels (same tiles, eps/beta per read)
+template <class W>
+struct WithGcp;
+template <int G, int R, bool MT>
+struct WithGcp<Fp64Wavefront<G, R, MT, false>> {
+    using type = Fp64Wavefront<G, R, MT, true>;
+};
+
 #define PHMM_FP64_DISPATCH(cls, EXPR)      \
     switch (cls) {                          \
         case 0: { using W = W64c0; EXPR; }  \
@@ -90,15 +100,23 @@ size_t fp64_smem_for() {
         default: { using W = W64c6; EXPR; } \
     }
 
+// the gcp twin has the same tables and ring, so the same shared memory
 size_t fp64_smem_bytes(int cls) { PHMM_FP64_DISPATCH(cls, return fp64_smem_for<W>()); }
 size_t fp64_scratch_bytes_per_row(int cls) { return cls == kFp64Classes - 1 ? 2 * sizeof(Border64) : 0; }
-const void* fp64_kernel(int cls) {
-    PHMM_FP64_DISPATCH(cls, return reinterpret_cast<const void*>(&fp64_rescue_kernel<W>));
+const void* fp64_kernel(int cls, bool gcp) {
+    PHMM_FP64_DISPATCH(cls, return gcp ? reinterpret_cast<const void*>(&fp64_rescue_kernel<typename WithGcp<W>::type>)
+                                       : reinterpret_cast<const void*>(&fp64_rescue_kernel<W>));
 }
 int fp64_per_warp(int cls) { PHMM_FP64_DISPATCH(cls, return W::NG); }
 
 cudaError_t launch_fp64_rescue(const Fp64LaunchArgs& a) {
     Border64* scr = a.cls == kFp64Classes - 1 ? static_cast<Border64*>(a.scratch) : nullptr;
+    if (a.gcp) {
+        PHMM_FP64_DISPATCH(a.cls, (fp64_rescue_kernel<typename WithGcp<W>::type>
+                                   <<<a.grid, kBlockThreads, fp64_smem_bytes(a.cls), a.stream>>>(
+                                       a.view, a.items, a.count, a.counter, scr, a.rows));
+                           return cudaGetLastError());
+    }
     PHMM_FP64_DISPATCH(a.cls, (fp64_rescue_kernel<W><<<a.grid, kBlockThreads, fp64_smem_bytes(a.cls), a.stream>>>(
                                    a.view, a.items, a.count, a.counter, scr, a.rows));
                        return cudaGetLastError());

@@ -30,6 +30,7 @@ struct PrepArgs {
     const uint8_t* hap_bases;
     const int64_t* hap_offsets;
     const int32_t* hap_lengths;
+    const uint8_t* gcp_quals;       // gcp mode only (else null)
     // index arrays (device, computed on the host)
     const int32_t* read_record;     // [num_reads]
     const int32_t* read_local;      // [num_reads] read index inside its record
@@ -43,6 +44,7 @@ struct PrepArgs {
     // outputs
     uint32_t* read_pack;
     uint8_t* hap_code;
+    uint8_t* read_gcp;              // [num_reads], gcp mode only (else null)
 };
 
 #ifdef PHMM_PREP_KERNELS_IMPL
@@ -72,6 +74,10 @@ __global__ void pack_reads_kernel(PrepArgs a) {
         const bool aligned = ((reinterpret_cast<uintptr_t>(rb) | reinterpret_cast<uintptr_t>(bq) |
                                reinterpret_cast<uintptr_t>(iq) | reinterpret_cast<uintptr_t>(dq)) & 3u) == 0;
         uint4* dst = reinterpret_cast<uint4*>(a.read_pack + a.read_start[i]);  // 16-byte aligned
+        if (a.read_gcp && lane == 0) {
+            const uint32_t g = L > 0 ? a.gcp_quals[src] : 10u;
+            a.read_gcp[i] = (uint8_t)(g > 127u ? 127u : g);
+        }
         for (int c = lane * 4; c < Lp; c += 128) {
             uint32_t w[4];
             if (aligned && c + 3 < L) {

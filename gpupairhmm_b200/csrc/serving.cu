@@ -54,6 +54,11 @@ pairhmm_status_t ServingQueue::submit(const pairhmm_batch_t& b, uint64_t* ticket
         error_ = "null haplotype arrays";
         return PAIRHMM_ERR_INVALID_ARGUMENT;
     }
+    const bool gcp = parent_.gcp();
+    if (gcp && x.num_reads > 0 && !b.gcp_quals) {
+        error_ = "gcp mode needs the gcp quality array";
+        return PAIRHMM_ERR_INVALID_ARGUMENT;
+    }
     auto r = std::make_shared<Region>();
     r->rpr.assign(b.reads_per_record, b.reads_per_record + b.num_records);
     r->hpr.assign(b.haps_per_record, b.haps_per_record + b.num_records);
@@ -68,12 +73,14 @@ pairhmm_status_t ServingQueue::submit(const pairhmm_batch_t& b, uint64_t* ticket
     r->bq.resize(total);
     r->iq.resize(total);
     r->dq.resize(total);
+    if (gcp) r->gq.resize(total);
     for (int64_t i = 0; i < x.num_reads; ++i) {
         const int64_t o = b.read_offsets[i], d = r->read_off[i], L = b.read_lengths[i];
         std::memcpy(&r->read_bases[d], b.read_bases + o, L);
         std::memcpy(&r->bq[d], b.base_quals + o, L);
         std::memcpy(&r->iq[d], b.ins_quals + o, L);
         std::memcpy(&r->dq[d], b.del_quals + o, L);
+        if (gcp) std::memcpy(&r->gq[d], b.gcp_quals + o, L);
     }
     total = 0;
     for (int64_t h = 0; h < x.num_haps; ++h) { r->hap_off[h] = total; total += b.hap_lengths[h]; }
@@ -98,6 +105,7 @@ pairhmm_status_t ServingQueue::submit(const pairhmm_batch_t& b, uint64_t* ticket
                 o.fp64_rescue = 1;
                 o.use_graphs = 1;
                 o.pipeline_chunks = 1;  // merged batches stay small: one pass
+                o.gcp = gcp ? 1 : 0;
                 auto e = std::make_unique<Engine>(o);
                 pairhmm_status_t is = e->init();
                 if (is == PAIRHMM_OK) is = e->set_tile_table(parent_.tile_table());
@@ -126,7 +134,7 @@ void ServingQueue::worker(int slot) {
     // they have grown to the slot's usual size
     std::vector<int32_t> rpr, hpr, rl, hl;
     std::vector<int64_t> ro, ho;
-    std::vector<uint8_t> rb, bq, iq, dq, hb;
+    std::vector<uint8_t> rb, bq, iq, dq, gq, hb;
     std::vector<float> scores;
     for (;;) {
         std::vector<std::shared_ptr<Region>> take;
@@ -153,7 +161,7 @@ void ServingQueue::worker(int slot) {
         for (auto* v : {&rpr, &hpr, &rl, &hl}) v->clear();
         ro.clear();
         ho.clear();
-        for (auto* v : {&rb, &bq, &iq, &dq, &hb}) v->clear();
+        for (auto* v : {&rb, &bq, &iq, &dq, &gq, &hb}) v->clear();
         for (const auto& r : take) {
             const int64_t rbase = (int64_t)rb.size(), hbase = (int64_t)hb.size();
             rpr.insert(rpr.end(), r->rpr.begin(), r->rpr.end());
@@ -166,6 +174,7 @@ void ServingQueue::worker(int slot) {
             bq.insert(bq.end(), r->bq.begin(), r->bq.end());
             iq.insert(iq.end(), r->iq.begin(), r->iq.end());
             dq.insert(dq.end(), r->dq.begin(), r->dq.end());
+            gq.insert(gq.end(), r->gq.begin(), r->gq.end());
             hb.insert(hb.end(), r->hap_bases.begin(), r->hap_bases.end());
         }
         pairhmm_batch_t b{};
@@ -176,6 +185,7 @@ void ServingQueue::worker(int slot) {
         b.base_quals = bq.data();
         b.ins_quals = iq.data();
         b.del_quals = dq.data();
+        b.gcp_quals = gq.empty() ? nullptr : gq.data();
         b.read_offsets = ro.data();
         b.read_lengths = rl.data();
         b.hap_bases = hb.data();

@@ -48,7 +48,7 @@ private:
         uint64_t ticket = 0;
         std::vector<int32_t> rpr, hpr, read_len, hap_len;
         std::vector<int64_t> read_off, hap_off;
-        std::vector<uint8_t> read_bases, bq, iq, dq, hap_bases;
+        std::vector<uint8_t> read_bases, bq, iq, dq, gq, hap_bases;  // gq: gcp mode only
         int64_t pairs = 0;
         int64_t device_bytes = 0;
         bool heavy = false;  // has a read beyond the largest single tile

@@ -46,6 +46,9 @@
 // consecutive float4s whatever codes the lanes hold (no bank conflicts) and a
 // thread only reads what it wrote (no synchronisation).
 //
+// GCP = true (gcp mode): eps and beta are the read's own instead of the
+// constants; everything else is the same.
+//
 // Reads longer than T (MT = true) run as several tiles; the last lane of tile
 // i writes (X^, I^, N) of its last position for every haplotype row into a
 // per-group scratch border, which lane 0 of tile i+1 reads as its left
@@ -56,7 +59,7 @@
 
 namespace phmm {
 
-template <int G, int R, bool MT>
+template <int G, int R, bool MT, bool GCP = false>
 struct Fp32Wavefront {
     static_assert(R % 4 == 0 && R >= 4, "R must be a multiple of 4");
     static_assert(G == 4 || G == 8 || G == 16 || G == 32, "G must divide the warp");
@@ -86,11 +89,17 @@ struct Fp32Wavefront {
 
         const uint32_t* rpack = v.read_pack + v.read_start[task.read];
         const uint32_t* hw = reinterpret_cast<const uint32_t*>(v.hap_code + v.hap_start[task.hap]);
-        const float Dbound = kBeta * (kScale / (float)Hc);
+        // eps and beta: the reference GPU path's constants, or in gcp mode the
+        // read's own from its first gcp quality, formed as the reference's CPU
+        // recurrence forms them (gpuworker.cuh:1048-1049)
+        const float eps = GCP ? ph[v.read_gcp[task.read]] : kEps;
+        const float beta = GCP ? (float)(1.0 - (double)eps) : kBeta;
+        const float Dbound = beta * (kScale / (float)Hc);
 
         float acc = 0.f;
         int rlane = -1;          // lane (in group) that holds the result
         bool degenerate = false; // some |alpha| < kMinAlpha: FP64 pass recomputes the pair
+        if (GCP && !(beta >= kMinAlpha)) degenerate = true;  // gcp quality 0: nothing to rescale by
 
         for (int tile = 0; tile < nt_warp; ++tile) {
             const bool tile_live = valid && tile < ntiles;
@@ -112,11 +121,11 @@ struct Fp32Wavefront {
             // column -1 (boundary values enter unscaled)
             float q_prev = 1.0f;
             if (p0 > 0) {
-                q_prev = kBeta;
+                q_prev = beta;
                 if (p0 - 1 < L) {
                     const uint32_t wp = __ldg(rpack + p0 - 1);
                     const float dp = ph[(wp >> 16) & 0x7fu];
-                    q_prev = (kBeta * dp) / (1.0f - (dp + ph[(wp >> 24) & 0x7fu]));
+                    q_prev = (beta * dp) / (1.0f - (dp + ph[(wp >> 24) & 0x7fu]));
                 }
             }
             float dpv[R], ee[R], rr[R];
@@ -158,10 +167,10 @@ struct Fp32Wavefront {
                     for (int h = 0; h < 5; ++h)
                         lam[h][s] = in ? an * ((x == 4u || h == 4 || x == (uint32_t)h) ? lm : lx) : 0.0f;
                     if (in && !(fabsf(a_cur[r]) >= kMinAlpha)) degenerate = true;
-                    const float qc = in ? (kBeta * d) / a_cur[r] : kBeta;  // I scale of c
+                    const float qc = in ? (beta * d) / a_cur[r] : beta;  // I scale of c
                     dpv[r] = qp;
-                    ee[r] = ((in ? kEps : 1.0f) * qp) / qc;
-                    rr[r] = in ? ((kBeta * sg) / an) / qc : 0.0f;
+                    ee[r] = ((in ? eps : 1.0f) * qp) / qc;
+                    rr[r] = in ? ((beta * sg) / an) / qc : 0.0f;
                     qp = qc;
                     N[r] = 0.0f;
                     D[r] = 0.0f;
@@ -185,7 +194,7 @@ struct Fp32Wavefront {
             const bool addM = r_res == R - 1;
             // weight of the lane's last I^ in the result: beta in the carry, q when
             // the read ends on the lane's last position
-            const float qres = addM ? q_last : kBeta;
+            const float qres = addM ? q_last : beta;
             if (res_lane) rlane = t;
             const int kmax = (int)__reduce_max_sync(kFullMask, (unsigned)(tile_live ? kg : 0));
             const int K = (kmax + 1 + 3) & ~3;
@@ -237,7 +246,7 @@ struct Fp32Wavefront {
                             const float Nold = N[r];
                             const float Dold = D[r];
                             N[r] = ls[u] * fmaf(dpv[r], Xdiag, Ndiag);
-                            D[r] = fmaf(kEps, Dold, Nold);
+                            D[r] = fmaf(eps, Dold, Nold);
                             // e*I^ carries the serial chain: one FFMA per position
                             const float In = fmaf(ee[r], Idiag, Ndiag);
                             Xdiag = fmaf(rr[r], Dold, In);
@@ -249,7 +258,7 @@ struct Fp32Wavefront {
                     // the read ends on the lane's last register
                     if (res_lane && k <= kg) {
                         acc = fmaf(qres, Idiag, acc);
-                        if (addM && k < kg) acc = fmaf(kBeta, N[R - 1], acc);
+                        if (addM && k < kg) acc = fmaf(beta, N[R - 1], acc);
                     }
                     if (MT && writer) {
                         // slot s holds X^(s+1), I^(s+1), N(s)
@@ -293,7 +302,7 @@ struct Fp32Wavefront {
         const unsigned gmask = (G == 32 ? kFullMask : ((1u << G) - 1u)) << (grp * G);
         degenerate = (dmask & gmask) != 0u;
         if (valid && t == rlane) {
-            const float res = log10f(acc) - (log10f(kScale) + log10f(kBeta));
+            const float res = log10f(acc) - (log10f(kScale) + log10f(beta));
             v.scores[task.out] = res;
             if (degenerate || (v.rescue_enabled && !(acc >= rescue_threshold(L, H) && acc <= FLT_MAX))) {
                 append_rescue(v, fp64_class(L), task);

@@ -54,7 +54,7 @@ __device__ __forceinline__ double pow2i(int k) {
     return __longlong_as_double((long long)(k + 1023) << 52);
 }
 
-template <int G, int R, bool MT>
+template <int G, int R, bool MT, bool GCP = false>
 struct Fp64Wavefront {
     static_assert(R % 2 == 0, "R must be even");
     static_assert(!MT || G == 32, "multi-tile FP64 runs one pair per warp");
@@ -81,8 +81,11 @@ struct Fp64Wavefront {
         const int ntiles = MT ? (Lc + T - 1) / T : 1;  // MT: one group, warp-uniform
         const uint32_t* rpack = v.read_pack + v.read_start[task.read];
         const uint32_t* hw = reinterpret_cast<const uint32_t*>(v.hap_code + v.hap_start[task.hap]);
-        const double beta = (double)kBeta;
-        const double epsd = (double)kEps;
+        // gcp mode: the read's own eps and beta (gpuworker.cuh:1048-1049), as the
+        // FP32 kernel forms them; beta = 0 (gcp quality 0) has no rescaled form
+        const float eps_f = GCP ? ph[v.read_gcp[task.read]] : kEps;
+        const double beta = GCP ? (double)(float)(1.0 - (double)eps_f) : (double)kBeta;
+        const double epsd = (double)eps_f;
         const double Dbound = beta * (double)(kScale / (float)Hc);
 
         double acc = 0.0;
@@ -265,8 +268,8 @@ struct Fp64Wavefront {
         if (valid && t == rlane) {
             double res = -INFINITY;
             if (acc > 0.0)
-                res = log10(acc) - (double)e * 0.30102999566398119521 - log10((double)kScale) -
-                      log10((double)kBeta);
+                res = log10(acc) - (double)e * 0.30102999566398119521 - log10((double)kScale) - log10(beta);
+            if (GCP && !(beta > 0.0)) res = NAN;
             v.scores[task.out] = (float)res;
         }
     }

@@ -101,7 +101,14 @@ typedef struct pairhmm_options {
     int32_t pipeline_chunks; /* compute_host: 0 (default) = batches of 4M+ pairs run as up to
                                 4 chunks whose uploads overlap the previous chunk's kernels;
                                 1 = one pass; N = N chunks */
-    int32_t reserved;        /* 0 */
+    int32_t gcp;             /* 0 (default): eps = 0.1, beta = 0.9 for every pair, as the reference's
+                                GPU path (pairhmm_kernels.cuh:1195-1196; gcp qualities unused).
+                                1: eps = p(gcp), beta = 1 - eps per read, from the gcp quality
+                                of its first position, as the reference's CPU path
+                                (gpuworker.cuh:1009, 1048-1049); the batch must carry
+                                gcp_quals, and a gcp quality of 0 (beta = 0) is rejected
+                                (compute_host) or scores NaN (compute_device).  Engine form
+                                only. */
 } pairhmm_options_t;
 
 typedef struct pairhmm_stats {

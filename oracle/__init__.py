@@ -49,6 +49,11 @@ def lib() -> ctypes.CDLL:
         L.oracle_pair_log10.argtypes = [ctypes.c_void_p] * 4 + [ctypes.c_int, ctypes.c_void_p, ctypes.c_int]
         L.oracle_batch_log10.restype = ctypes.c_int64
         L.oracle_batch_log10.argtypes = [ctypes.c_int64] + [ctypes.c_void_p] * 11 + [ctypes.c_void_p, ctypes.c_int]
+        L.oracle_batch_log10_gcp.restype = ctypes.c_int64
+        L.oracle_batch_log10_gcp.argtypes = [ctypes.c_int64] + [ctypes.c_void_p] * 12 + [ctypes.c_void_p, ctypes.c_int]
+        L.oracle_pair_log10_gcp.restype = ctypes.c_double
+        L.oracle_pair_log10_gcp.argtypes = [ctypes.c_void_p] * 4 + [ctypes.c_int, ctypes.c_void_p, ctypes.c_int,
+                                                                    ctypes.c_int]
         L.oracle_ph2pr.restype = ctypes.c_float
         L.oracle_ph2pr.argtypes = [ctypes.c_int]
         L.oracle_max_threads.restype = ctypes.c_int
@@ -89,11 +94,13 @@ def pair_log10(read: bytes, bq, iq, dq, hap: bytes) -> float:
     return lib().oracle_pair_log10(_ptr(r), _ptr(b), _ptr(i), _ptr(d), len(r), _ptr(h), len(h))
 
 
-def batch_log10(batch, nthreads: int = 0) -> np.ndarray:
+def batch_log10(batch, nthreads: int = 0, gcp: bool = False) -> np.ndarray:
     """FP64 log10 likelihood per pair for a batch object exposing the SoA arrays
     (``reads_per_record``, ``haps_per_record``, ``read_bases``, ``base_quals``,
     ``ins_quals``, ``del_quals``, ``read_offsets``, ``read_lengths``,
-    ``hap_bases``, ``hap_offsets``, ``hap_lengths``)."""
+    ``hap_bases``, ``hap_offsets``, ``hap_lengths``).  gcp=True takes eps and
+    beta per read from ``gcp_quals`` at its first position (the product's gcp
+    mode); otherwise the GPU path's constants."""
     rpr = np.ascontiguousarray(batch.reads_per_record, dtype=np.int32)
     hpr = np.ascontiguousarray(batch.haps_per_record, dtype=np.int32)
     arrs = [np.ascontiguousarray(getattr(batch, n), dtype=np.uint8)
@@ -106,6 +113,11 @@ def batch_log10(batch, nthreads: int = 0) -> np.ndarray:
     npairs = int((rpr.astype(np.int64) * hpr).sum())
     out = np.empty(npairs, dtype=np.float64)
     if npairs == 0:
+        return out
+    if gcp:
+        gq = np.ascontiguousarray(batch.gcp_quals, dtype=np.uint8)
+        lib().oracle_batch_log10_gcp(len(rpr), _ptr(rpr), _ptr(hpr), *[_ptr(a) for a in arrs], _ptr(gq),
+                                     _ptr(ro), _ptr(rl), _ptr(hb), _ptr(ho), _ptr(hl), _ptr(out), int(nthreads))
         return out
     lib().oracle_batch_log10(len(rpr), _ptr(rpr), _ptr(hpr), *[_ptr(a) for a in arrs],
                              _ptr(ro), _ptr(rl), _ptr(hb), _ptr(ho), _ptr(hl), _ptr(out), int(nthreads))

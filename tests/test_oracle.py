@@ -99,3 +99,68 @@ def test_oracle_batch_order_matches_pairwise():
         ri += R
         hi += H
     assert k == len(full)
+
+
+def _pair_gcp(read, bq, iq, dq, hap, gcp):
+    r = np.frombuffer(bytes(read), np.uint8).copy()
+    h = np.frombuffer(bytes(hap), np.uint8).copy()
+    return oracle.lib().oracle_pair_log10_gcp(r.ctypes.data, bq.ctypes.data, iq.ctypes.data, dq.ctypes.data,
+                                              len(r), h.ctypes.data, len(h), int(gcp))
+
+
+def test_oracle_gcp_mode_matches_reference_align_host():
+    """gcp mode takes eps = p(gcp) and beta = 1 - eps from the read's first gcp
+    quality: the reference's CPU recurrence (gpuworker.cuh:1009, 1048-1049)."""
+    ref = oracle.ref_cpu()
+    if ref is None:
+        pytest.skip("reference shim not built (no reference sources here)")
+    rng = np.random.default_rng(99)
+    got, want = [], []
+    for i in range(300):
+        L = int(rng.integers(1, 160))
+        H = int(rng.integers(1, 260))
+        read, bq, iq, dq, hap = _rand_pair(rng, L, H)
+        if i % 4 and H > L:
+            s = int(rng.integers(0, H - L + 1))
+            read = hap[s:s + L]
+        gcp = int(rng.integers(1, 45))
+        o = _pair_gcp(read, bq, iq, dq, hap, gcp)
+        r = ref.ref_align_host(np.frombuffer(hap, np.uint8).ctypes.data, H,
+                               np.frombuffer(read, np.uint8).ctypes.data, L,
+                               bq.ctypes.data, iq.ctypes.data, dq.ctypes.data, gcp)
+        if r > -60.0:
+            got.append(o)
+            want.append(r)
+    assert len(got) > 150
+    assert_log10_close(got, want, what="oracle gcp mode vs align_host")
+
+
+def test_oracle_gcp_mode_batch():
+    """Per read, the first position's gcp quality decides; gcp 10 everywhere is
+    the GPU path's eps 0.1 and beta 0.9 exactly."""
+    from gpupairhmm_b200 import synth
+    b = synth.config0(seed=4, records=3)
+    default = oracle.batch_log10(b)
+    assert np.array_equal(oracle.batch_log10(b, gcp=True), default)  # synthetic gcp is 10
+    rng = np.random.default_rng(5)
+    gq = rng.integers(1, 41, size=len(b.gcp_quals)).astype(np.uint8)
+    b2 = type(b)(**{**b.__dict__, "gcp_quals": gq})
+    full = oracle.batch_log10(b2, gcp=True)
+    k = 0
+    ri, hi = 0, 0
+    for g in range(b.num_records):
+        R, H = int(b.reads_per_record[g]), int(b.haps_per_record[g])
+        for r in range(R):
+            o, L = int(b.read_offsets[ri + r]), int(b.read_lengths[ri + r])
+            for h in range(H):
+                ho, hn = int(b.hap_offsets[hi + h]), int(b.hap_lengths[hi + h])
+                v = _pair_gcp(bytes(b.read_bases[o:o + L]), b.base_quals[o:o + L], b.ins_quals[o:o + L],
+                              b.del_quals[o:o + L], bytes(b.hap_bases[ho:ho + hn]), int(gq[o]))
+                assert v == full[k]
+                k += 1
+        ri += R
+        hi += H
+    assert not np.array_equal(full, default)
+    ref = oracle.ref_cpu()
+    if ref is not None:  # the reference's own batch loop over the same gcp array
+        assert_log10_close(full, oracle.ref_batch_log10(b2), what="oracle gcp batch vs reference CPU batch")
