@@ -12,7 +12,10 @@ Outputs:
   gpupairhmm_b200/tuning_sm100a.json   every measurement and the table
   gpupairhmm_b200/csrc/tuned_table.inc the table compiled into the engine
 
-  python -m gpupairhmm_b200.autotune [--pairs-per-class N] [--repeats K]
+  python -m gpupairhmm_b200.autotune [--pairs-per-class N] [--repeats K] [--only LO-HI]
+
+--only re-times the classes inside [LO, HI] and keeps the earlier measurements
+of the others (from tuning_sm100a.json) when it rebuilds the table.
 """
 from __future__ import annotations
 
@@ -30,6 +33,8 @@ HERE = Path(__file__).resolve().parent
 
 SINGLE = [(G, R) for G in (4, 8, 16, 32) for R in (4, 8, 12, 16, 20, 24, 28, 32)
           if not (G >= 8 and R == 4)]
+# tiles with R % 4 == 2 where G*R falls on a class bound that no other tile has
+SINGLE += [(8, 14), (8, 18), (8, 22), (16, 10), (16, 14), (16, 18)]
 MULTI = [(32, 16), (32, 20), (32, 24), (32, 28), (32, 32), (16, 32)]
 PACKED = [(G, R) for G in (4, 8, 16, 32) for R in (8, 12, 16)]  # two reads per group, packed FP32
 
@@ -78,11 +83,13 @@ def time_config(engine: Engine, batch: Batch, G: int, R: int, kind: int, repeats
     return best
 
 
-def tune(pairs_per_class: int = 60000, repeats: int = 3, device: int = 0):
+def tune(pairs_per_class: int = 60000, repeats: int = 3, device: int = 0, only=None):
     eng = Engine(device=device, fp64_rescue=False)
     eng.set_tile_table([(1 << 30, 32, 32, 1)])
     results = []
     for ci, (lo, hi) in enumerate(classes()):
+        if only and not (only[0] <= lo and hi <= only[1]):
+            continue
         batch = class_batch(lo, hi, pairs_per_class if hi <= 1024 else max(512, pairs_per_class // 8), 1000 + ci)
         cands = [(G, R, 0) for G, R in SINGLE if G * R >= hi] if hi <= 1024 else []
         cands += [(G, R, 2) for G, R in PACKED if G * R >= hi]
@@ -137,8 +144,14 @@ def main():
     ap.add_argument("--repeats", type=int, default=3)
     ap.add_argument("--device", type=int, default=0)
     ap.add_argument("--outdir", default=None, help="also copy the outputs here")
+    ap.add_argument("--only", default=None, help="LO-HI: re-time only the classes inside, keep the others")
     a = ap.parse_args()
-    res = tune(a.pairs_per_class, a.repeats, a.device)
+    only = tuple(int(x) for x in a.only.split("-")) if a.only else None
+    res = tune(a.pairs_per_class, a.repeats, a.device, only)
+    if only:  # merge with the earlier measurements of the other classes
+        new = {(r["lo"], r["hi"]): r for r in res}
+        old = json.loads((HERE / "tuning_sm100a.json").read_text())["classes"]
+        res = [new.get((r["lo"], r["hi"]), r) for r in old]
     rules = to_rules(res)
     write_outputs(res, rules)
     print("rules:", rules)

@@ -15,6 +15,7 @@ void register_fp32_g8(std::vector<ConfigInfo>& out);
 void register_fp32_g16(std::vector<ConfigInfo>& out);
 void register_fp32_g32(std::vector<ConfigInfo>& out);
 void register_fp32_gcp(std::vector<ConfigInfo>& out);
+void register_fp32_geven(std::vector<ConfigInfo>& out);
 
 const std::vector<ConfigInfo>& fp32_configs() {
     static std::vector<ConfigInfo> all;
@@ -24,6 +25,7 @@ const std::vector<ConfigInfo>& fp32_configs() {
         register_fp32_g8(all);
         register_fp32_g16(all);
         register_fp32_g32(all);
+        register_fp32_geven(all);
         register_fp32_gcp(all);
     });
     return all;

@@ -44,7 +44,10 @@
 // lam' table: each thread owns 5 x R floats in shared memory, laid out as
 // [hap code][R/4][32 lanes] float4, so a warp-wide 16-byte load touches 32
 // consecutive float4s whatever codes the lanes hold (no bank conflicts) and a
-// thread only reads what it wrote (no synchronisation).
+// thread only reads what it wrote (no synchronisation).  With R % 4 == 2 the
+// last two positions of each code follow as a [hap code][32 lanes] float2
+// table (a 150-position read fits 8 x 18 = 144 + one more tile row instead of
+// 8 x 20 = 160: fewer padded cells for the common 129-144 lengths).
 //
 // GCP = true (gcp mode): eps and beta are the read's own instead of the
 // constants; everything else is the same.
@@ -61,12 +64,40 @@ namespace phmm {
 
 template <int G, int R, bool MT, bool GCP = false>
 struct Fp32Wavefront {
-    static_assert(R % 4 == 0 && R >= 4, "R must be a multiple of 4");
+    static_assert(R % 2 == 0 && R >= 4, "R must be even");
     static_assert(G == 4 || G == 8 || G == 16 || G == 32, "G must divide the warp");
     static constexpr int NG = 32 / G;   // pairs per warp
     static constexpr int T = G * R;     // read positions per tile
     static constexpr int Q = R / 4;     // float4 per thread per table row
-    static constexpr int kTableFloat4 = 5 * Q * 32;  // per warp
+    static constexpr bool kTail = R % 4 == 2;       // then one float2 group after them
+    static constexpr int NGRP = Q + (kTail ? 1 : 0);  // position groups: 4 each, the tail 2
+    static constexpr int kTail2 = 5 * Q * 32;       // float4 index where the float2 tail table starts
+    static constexpr int kTableFloat4 = 5 * Q * 32 + (kTail ? 5 * 32 / 2 : 0);  // per warp
+
+    __host__ __device__ static constexpr int group_size(int g) { return g < Q ? 4 : 2; }
+
+    // Packed words of position group g of the lane starting at p0 (zero past the
+    // read's padded end).  A lane starts at a multiple of R positions, so with
+    // R % 4 == 2 its groups are only 8-byte aligned and load as uint2 pairs.
+    __device__ __forceinline__ static void load_group(const uint32_t* rpack, int p0, int g, int Lc,
+                                                      uint32_t (&ws)[4]) {
+        ws[0] = ws[1] = ws[2] = ws[3] = 0u;
+        const int p = p0 + 4 * g;
+        if (p >= Lc) return;
+        if (g < Q) {
+            if constexpr (R % 4 == 0) {
+                const uint4 w = __ldg(reinterpret_cast<const uint4*>(rpack + p));
+                ws[0] = w.x; ws[1] = w.y; ws[2] = w.z; ws[3] = w.w;
+            } else {
+                const uint2 a = __ldg(reinterpret_cast<const uint2*>(rpack + p));
+                const uint2 b = __ldg(reinterpret_cast<const uint2*>(rpack + p + 2));
+                ws[0] = a.x; ws[1] = a.y; ws[2] = b.x; ws[3] = b.y;
+            }
+        } else {
+            const uint2 a = __ldg(reinterpret_cast<const uint2*>(rpack + p));
+            ws[0] = a.x; ws[1] = a.y;
+        }
+    }
 
     // items: the warp's ntask (<= NG) work items (read1 unused).  wtab: this warp's table
     // (kTableFloat4 float4).  ph: 128-entry probability table (shared).
@@ -132,13 +163,12 @@ struct Fp32Wavefront {
             float N[R], D[R];
             float a_cur[R];
 #pragma unroll
-            for (int q = 0; q < Q; ++q) {
-                uint4 w = make_uint4(0u, 0u, 0u, 0u);
-                if (p0 + 4 * q < Lc) w = __ldg(reinterpret_cast<const uint4*>(rpack + p0 + 4 * q));
-                const uint32_t ws[4] = {w.x, w.y, w.z, w.w};
+            for (int g = 0; g < NGRP; ++g) {
+                uint32_t ws[4];
+                load_group(rpack, p0, g, Lc, ws);
 #pragma unroll
-                for (int s = 0; s < 4; ++s) {
-                    const int r = 4 * q + s;
+                for (int s = 0; s < group_size(g); ++s) {
+                    const int r = 4 * g + s;
                     const float d = ph[(ws[s] >> 16) & 0x7fu];
                     const float sg = ph[(ws[s] >> 24) & 0x7fu];
                     a_cur[r] = (p0 + r < L) ? 1.0f - (d + sg) : 1.0f;  // pairhmm_kernels.cuh:1336
@@ -146,14 +176,13 @@ struct Fp32Wavefront {
             }
             float qp = q_prev;
 #pragma unroll
-            for (int q = 0; q < Q; ++q) {
-                uint4 w = make_uint4(0u, 0u, 0u, 0u);
-                if (p0 + 4 * q < Lc) w = __ldg(reinterpret_cast<const uint4*>(rpack + p0 + 4 * q));
-                const uint32_t ws[4] = {w.x, w.y, w.z, w.w};
+            for (int g = 0; g < NGRP; ++g) {
+                uint32_t ws[4];
+                load_group(rpack, p0, g, Lc, ws);
                 float lam[5][4];
 #pragma unroll
-                for (int s = 0; s < 4; ++s) {
-                    const int r = 4 * q + s;
+                for (int s = 0; s < group_size(g); ++s) {
+                    const int r = 4 * g + s;
                     const int c = p0 + r;
                     const uint32_t x = ws[s] & 0xffu;
                     const float p = ph[(ws[s] >> 8) & 0x7fu];
@@ -176,8 +205,12 @@ struct Fp32Wavefront {
                     D[r] = 0.0f;
                 }
 #pragma unroll
-                for (int h = 0; h < 5; ++h)
-                    wtab[(h * Q + q) * 32 + lane] = make_float4(lam[h][0], lam[h][1], lam[h][2], lam[h][3]);
+                for (int h = 0; h < 5; ++h) {
+                    if (g < Q)
+                        wtab[(h * Q + g) * 32 + lane] = make_float4(lam[h][0], lam[h][1], lam[h][2], lam[h][3]);
+                    else
+                        reinterpret_cast<float2*>(wtab + kTail2)[h * 32 + lane] = make_float2(lam[h][0], lam[h][1]);
+                }
             }
             const float q_last = qp;  // I scale of this lane's last position
 
@@ -237,12 +270,18 @@ struct Fp32Wavefront {
                     const float4* trow = wtab + h * (Q * 32) + lane;
                     float Ndiag = Mul, Idiag = Iul, Xdiag = Xul;
 #pragma unroll
-                    for (int q = 0; q < Q; ++q) {
-                        const float4 lam = trow[q * 32];
-                        const float ls[4] = {lam.x, lam.y, lam.z, lam.w};
+                    for (int g = 0; g < NGRP; ++g) {
+                        float ls[4];
+                        if (g < Q) {
+                            const float4 lam = trow[g * 32];
+                            ls[0] = lam.x; ls[1] = lam.y; ls[2] = lam.z; ls[3] = lam.w;
+                        } else {
+                            const float2 lam = reinterpret_cast<const float2*>(wtab + kTail2)[h * 32 + lane];
+                            ls[0] = lam.x; ls[1] = lam.y; ls[2] = ls[3] = 0.0f;
+                        }
 #pragma unroll
-                        for (int u = 0; u < 4; ++u) {
-                            const int r = 4 * q + u;
+                        for (int u = 0; u < group_size(g); ++u) {
+                            const int r = 4 * g + u;
                             const float Nold = N[r];
                             const float Dold = D[r];
                             N[r] = ls[u] * fmaf(dpv[r], Xdiag, Ndiag);

@@ -73,6 +73,23 @@ def test_length_sweep_across_tile_boundaries(engine, plain_engine):
     assert_log10_close(plain_engine.compute(b)[ok], want[ok], what="sweep plain")
 
 
+@pytest.mark.parametrize("G,R", [(8, 14), (8, 18), (8, 22), (16, 10), (16, 14), (16, 18)])
+def test_even_r_tiles_match_oracle(G, R):
+    """Tiles with R % 4 == 2 (lanes start 8-byte aligned, a float2 tail table):
+    read lengths at every lane and tile edge of the tile."""
+    rng = np.random.default_rng(60 + G + R)
+    T = G * R
+    lens = sorted({1, 2, 3, R - 2, R - 1, R, R + 1, R + 2, 2 * R - 1, 2 * R, 2 * R + 1, T // 2 - 1, T // 2,
+                   T - 3, T - 2, T - 1, T})
+    recs = [_record(rng, L, int(rng.integers(max(L, 8), L + 300)), n_reads=2, n_haps=2) for L in lens]
+    b = _soa(recs)
+    e = g.Engine()
+    e.set_tile_table([(T, G, R, 0), (1 << 30, 32, 32, 1)])
+    got = e.compute(b)
+    e.close()
+    assert_log10_close(got, oracle.batch_log10(b), what=f"{G}x{R} tile")
+
+
 def test_haplotype_length_sweep(engine):
     rng = np.random.default_rng(6)
     recs = [_record(rng, 100, H, n_reads=3, n_haps=2) for H in
