@@ -50,7 +50,7 @@ static_assert(W64c0::T == kFp64ClassMax[0] && W64c1::T == kFp64ClassMax[1] && W6
               "class bounds follow the tiles");
 
 template <class W>
-__global__ void __launch_bounds__(kBlockThreads)
+__global__ void __launch_bounds__(kBlockThreads, W::kMinCtas)
 fp64_rescue_kernel(DevView v, const Task* __restrict__ items, const unsigned long long* count,
                    unsigned long long* counter, Border64* scratch, int64_t rows) {
     extern __shared__ double2 smem64[];

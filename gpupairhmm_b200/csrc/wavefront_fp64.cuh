@@ -63,6 +63,11 @@ struct Fp64Wavefront {
     static constexpr int Q = R / 2;                   // double2 per thread per table row
     static constexpr int kTableDouble2 = 5 * Q * 32;  // per warp
     static constexpr int kRing = 32;
+    // resident 64-thread CTAs per SM asked of the register allocator: the
+    // 10-position tile allocates about 200 registers (2 warps per scheduler),
+    // capped at 168 it keeps 3; the 8-position single tiles allocate about 158,
+    // capped at 128 they keep 4
+    static constexpr int kMinCtas = R == 10 ? 6 : (R == 8 && !MT) ? 8 : 1;
 
     // tasks: the warp's ntask (<= NG) items.  wtab: this warp's lambda table;
     // ring: kRing shared entries (MT); scratch: this warp's 2 x rows Border64.
