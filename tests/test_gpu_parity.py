@@ -186,6 +186,22 @@ def test_fp64_long_reads_short_haplotypes(engine):
     assert_log10_close(engine.compute(b), want, what="long reads, short haplotypes")
 
 
+def test_fp64_multi_tile_lengths(engine):
+    """FP64 multi-tile pairs (256-position tiles, border rows through global
+    memory): lengths at the single-tile bound and at 2, 3, 8, 9, 16 and 17+
+    tiles, against haplotypes from 1 to 1,500 positions."""
+    rng = np.random.default_rng(23)
+    recs = [_record(rng, L, H, n_reads=2, n_haps=2, bq=(35, 42), related=False)
+            for L, H in [(512, 300), (513, 300), (768, 60), (769, 2), (2048, 400), (2049, 9), (2300, 1500),
+                         (4097, 120), (4500, 33)]]
+    b = _soa(recs)
+    want = oracle.batch_log10(b)
+    got = engine.compute(b)
+    assert engine.stats().rescued >= len(want) - 4  # unrelated high-quality reads: FP64 throughout
+    assert np.isfinite(got).all()
+    assert_log10_close(got, want, what="FP64 multi-tile lengths")
+
+
 def test_empty_and_ragged_records(engine):
     rng = np.random.default_rng(15)
     from oracle.formats import Record
