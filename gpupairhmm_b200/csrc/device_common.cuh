@@ -91,7 +91,7 @@ __device__ __forceinline__ uint32_t code_of(uint8_t c) {
 __device__ __forceinline__ int min_i(int a, int b) { return a < b ? a : b; }
 
 // FP64 pass length classes (tile = G x R): 64 = 4x16, 96 = 8x12, 128 = 8x16,
-// 160 = 16x10, 192 = 16x12, 256 = 16x16, then 32x8 multi-tile for longer reads.
+// 160 = 16x10, 192 = 16x12, 256 = 16x16, then 32x16 multi-tile for longer reads.
 constexpr int kFp64Classes = 7;
 constexpr int kFp64ClassMax[kFp64Classes - 1] = {64, 96, 128, 160, 192, 256};
 __host__ __device__ __forceinline__ int fp64_class(int L) {

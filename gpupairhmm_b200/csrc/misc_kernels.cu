@@ -43,13 +43,16 @@ const ConfigInfo* find_fp32_config(int G, int R, bool multi_tile, bool packed, b
 // positions per lane where the registers allow (2 warps per scheduler at
 // 216-255 registers beat 4 warps at 8 positions: FP64 pass of the uneven
 // workload -6%, of 250-bp reads -9%); 160 keeps 16 x 10 at 168 registers.
+// Multi-tile: 512-row tiles (32 x 16) halve the tiles of a long pair against
+// 32 x 8 (long-read workload's FP64 pass 38.3 -> 26.9 ms; one long-read
+// region's 11.5 -> 7.3 ms).
 using W64c0 = Fp64Wavefront<4, 16, false>;
 using W64c1 = Fp64Wavefront<8, 12, false>;
 using W64c2 = Fp64Wavefront<8, 16, false>;
 using W64c3 = Fp64Wavefront<16, 10, false>;
 using W64c4 = Fp64Wavefront<16, 12, false>;
 using W64c5 = Fp64Wavefront<16, 16, false>;
-using W64c6 = Fp64Wavefront<32, 8, true>;
+using W64c6 = Fp64Wavefront<32, 16, true>;
 static_assert(W64c0::T == kFp64ClassMax[0] && W64c1::T == kFp64ClassMax[1] && W64c2::T == kFp64ClassMax[2] &&
                   W64c3::T == kFp64ClassMax[3] && W64c4::T == kFp64ClassMax[4] && W64c5::T == kFp64ClassMax[5],
               "class bounds follow the tiles");

@@ -187,9 +187,9 @@ def test_fp64_long_reads_short_haplotypes(engine):
 
 
 def test_fp64_multi_tile_lengths(engine):
-    """FP64 multi-tile pairs (256-position tiles, border rows through global
-    memory): lengths at the single-tile bound and at 2, 3, 8, 9, 16 and 17+
-    tiles, against haplotypes from 1 to 1,500 positions."""
+    """FP64 multi-tile pairs (512-position tiles, border rows through global
+    memory): lengths at the single-tile bound and at 1 to 9 tiles, against
+    haplotypes from 1 to 1,500 positions."""
     rng = np.random.default_rng(23)
     recs = [_record(rng, L, H, n_reads=2, n_haps=2, bq=(35, 42), related=False)
             for L, H in [(512, 300), (513, 300), (768, 60), (769, 2), (2048, 400), (2049, 9), (2300, 1500),
