@@ -37,6 +37,8 @@
 // buffer, staged through a 32-entry shared ring for lane 0 of the next tile.
 #pragma once
 
+#include <climits>
+
 #include "device_common.cuh"
 
 namespace phmm {
@@ -63,6 +65,10 @@ struct Fp64Wavefront {
     static constexpr int Q = R / 2;                   // double2 per thread per table row
     static constexpr int kTableDouble2 = 5 * Q * 32;  // per warp
     static constexpr int kRing = 32;
+    // largest scale difference a hand-off converts: stored values stay within
+    // about 2^(64 + 13*16) of 1 between renormalisations, so 2^640 more keeps
+    // every converted value below 2^1023
+    static constexpr int kMaxShift = 640;
     // resident 64-thread CTAs per SM asked of the register allocator: the
     // 10-position tile allocates about 200 registers (2 warps per scheduler),
     // capped at 168 it keeps 3; the 8-position single tiles allocate about 158,
@@ -193,6 +199,23 @@ struct Fp64Wavefront {
                         empty = false;
                     }
                     const double2* trow = wtab + h * (Q * 32) + lane;
+                    {
+                        // a neighbour's values far above this lane's scale (a lane centred on
+                        // the tiny first values of a long insertion path meets the large ones
+                        // that follow): coarsen the scale first, by an exact power of two, so
+                        // the conversion below cannot overflow; this lane's values that fall
+                        // out of range are negligible next to the incoming ones
+                        const int dM = Mul != 0.0 ? e - eMul : INT_MIN;
+                        const int dI = (Xul != 0.0 || Iul != 0.0) ? e - eIul : INT_MIN;
+                        const int over = (dM > dI ? dM : dI) - kMaxShift;
+                        if (over > 0) {
+                            const double f = over > 1022 ? 0.0 : pow2i(-over);
+#pragma unroll
+                            for (int r = 0; r < R; ++r) { M[r] *= f; D[r] *= f; }
+                            acc *= f;
+                            e -= over;
+                        }
+                    }
                     const double fM = pow2i(e - eMul);
                     const double fI = pow2i(e - eIul);
                     double Mdiag = Mul * fM;
@@ -249,7 +272,9 @@ struct Fp64Wavefront {
                     // renormalise every 16 steps (exact powers of two); a value moves by at
                     // most 2^13 per row, so lanes stay within 2^300 of their scale meanwhile
                     if ((k & 15) == 15) {
-                        double mx = res_lane ? fabs(acc) : 0.0;
+                        // the hand-off values count too: past the read end M is zero and
+                        // only the carried I^ and X^ move
+                        double mx = fmax(res_lane ? fabs(acc) : 0.0, fmax(fabs(Idiag), fabs(Xdiag)));
 #pragma unroll
                         for (int r = 0; r < R; ++r) mx = fmax(mx, fmax(fabs(M[r]), fabs(D[r])));
                         if (mx > 0.0) {
