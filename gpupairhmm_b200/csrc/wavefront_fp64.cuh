@@ -101,6 +101,7 @@ struct Fp64Wavefront {
 
         double acc = 0.0;
         int e = 0;
+        int eacc = 0;  // exponent of acc: the lane's e up to the pair's last step, then frozen
         int rlane = -1;
 
         for (int tile = 0; tile < ntiles; ++tile) {
@@ -199,7 +200,7 @@ struct Fp64Wavefront {
                         empty = false;
                     }
                     const double2* trow = wtab + h * (Q * 32) + lane;
-                    {
+                    if (e - (eMul < eIul ? eMul : eIul) > kMaxShift) {  // rare: one compare per step
                         // a neighbour's values far above this lane's scale (a lane centred on
                         // the tiny first values of a long insertion path meets the large ones
                         // that follow): coarsen the scale first, by an exact power of two, so
@@ -212,7 +213,7 @@ struct Fp64Wavefront {
                             const double f = over > 1022 ? 0.0 : pow2i(-over);
 #pragma unroll
                             for (int r = 0; r < R; ++r) { M[r] *= f; D[r] *= f; }
-                            acc *= f;
+                            if (k <= kg) acc *= f;
                             e -= over;
                         }
                     }
@@ -274,7 +275,7 @@ struct Fp64Wavefront {
                     if ((k & 15) == 15) {
                         // the hand-off values count too: past the read end M is zero and
                         // only the carried I^ and X^ move
-                        double mx = fmax(res_lane ? fabs(acc) : 0.0, fmax(fabs(Idiag), fabs(Xdiag)));
+                        double mx = fmax(res_lane && k <= kg ? fabs(acc) : 0.0, fmax(fabs(Idiag), fabs(Xdiag)));
 #pragma unroll
                         for (int r = 0; r < R; ++r) mx = fmax(mx, fmax(fabs(M[r]), fabs(D[r])));
                         if (mx > 0.0) {
@@ -284,11 +285,15 @@ struct Fp64Wavefront {
                                 const double f = pow2i(kk);
 #pragma unroll
                                 for (int r = 0; r < R; ++r) { M[r] *= f; D[r] *= f; }
-                                acc *= f;
+                                if (k <= kg) acc *= f;
                                 e += kk;
                             }
                         }
                     }
+                    // a group whose pair has ended keeps stepping while another group of
+                    // the warp runs on; its values then are not the pair's and must not
+                    // rescale the finished sum
+                    if (k <= kg) eacc = e;
                 }
                 wcur = wnext;
                 wnext = wpref;
@@ -298,7 +303,7 @@ struct Fp64Wavefront {
         if (valid && t == rlane) {
             double res = -INFINITY;
             if (acc > 0.0)
-                res = log10(acc) - (double)e * 0.30102999566398119521 - log10((double)kScale) - log10(beta);
+                res = log10(acc) - (double)eacc * 0.30102999566398119521 - log10((double)kScale) - log10(beta);
             if (GCP && !(beta > 0.0)) res = NAN;
             v.scores[task.out] = (float)res;
         }
