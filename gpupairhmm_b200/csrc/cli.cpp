@@ -4,14 +4,16 @@
 //
 //   pairhmm_b200 --inputfile in.txt --outputfile out.txt
 //                [--fileBatchsize N] [--transferBatchsize N] [--queue_depth N]
-//                [--verbose] [--checkResults] [--mode engine|plain] [--hostThreads N]
+//                [--verbose] [--checkResults] [--mode engine|plain] [--hostThreads N] [--gcp]
 //
 // fileBatchsize: minimum pairs per parsed batch; transferBatchsize: minimum
 // pairs per engine call inside a batch; a value <= 0 means unlimited
 // (main.cu:77-83).  Defaults follow the reference's code: 1,000,000 and
 // 10,000,000 (common.cuh:19-20).  --checkResults is accepted and, as in the
 // reference, has no effect.  --hostThreads sets the threads that parse and
-// format the text (default: all hardware threads).
+// format the text (default: all hardware threads).  --gcp takes eps and beta
+// per read from its first gcp quality, as the reference's CPU path does
+// (gpuworker.cuh:1009, 1048-1049), instead of the GPU path's 0.1 and 0.9.
 #include <atomic>
 #include <chrono>
 #include <condition_variable>
@@ -39,6 +41,7 @@ struct Options {
     int64_t fileBatchsize = 10000000;
     int queue_depth = 3;
     int mode = PAIRHMM_MODE_ENGINE;
+    bool gcp = false;
     std::string inputfile;
     std::string outputfile;
 };
@@ -114,6 +117,7 @@ void gpu_thread(const Options& o, Queue<PipelineData*>* in, Queue<PipelineData*>
     pairhmm_options_t eo;
     pairhmm_default_options(&eo);
     eo.mode = o.mode;
+    eo.gcp = o.gcp ? 1 : 0;
     pairhmm_engine_t* eng = nullptr;
     const auto t_engine = std::chrono::steady_clock::now();
     pairhmm_status_t st = pairhmm_engine_create(&eo, &eng);
@@ -222,6 +226,7 @@ int main(int argc, char** argv) {
         else if (a == "--queue_depth") o.queue_depth = std::atoi(val("--queue_depth").c_str());
         else if (a == "--checkResults") o.checkResults = true;
         else if (a == "--hostThreads") pairhmm_set_host_threads(std::atoi(val("--hostThreads").c_str()));
+        else if (a == "--gcp") o.gcp = true;
         else if (a == "--verbose") o.verbose = true;
         else if (a == "--mode") {
             const std::string m = val("--mode");
