@@ -208,8 +208,8 @@ def run_reference(args, cfg):
 def run_binary(args, cfg):
     """A gpuPairHMM-style binary on a record file of the workload (file parse,
     upload, compute, download; output to /dev/null as the reference skips
-    formatting for it).  GCUPS as printed by the binary.  One more run writes
-    the scores to a regular file and is timed whole (`file_to_file`)."""
+    formatting for it).  GCUPS as printed by the binary.  Three more runs write
+    the scores to a regular file and are timed whole (`file_to_file`, median)."""
     import re
     from gpupairhmm_b200 import synth, CLI_PATH
     binary = ROOT / "oracle" / "_ref" / "gpuPairHMM" if args.impl == "reference-gpu" else CLI_PATH
@@ -230,15 +230,26 @@ def run_binary(args, cfg):
             m = re.search(r"Batch processing time: ([0-9.e+-]+)s \(([0-9.e+-]+) GCUPS\)", out)
             if i >= args.warmup:
                 vals.append((float(m.group(1)), float(m.group(2))))
-        # the whole command once more with a regular output file: process start,
-        # parse, compute and the "%.5f" text, by the wall clock around it
+        # the whole command three times more with a regular output file: process
+        # start, parse, compute and the "%.5f" text, by the wall clock around it
+        # (median; our CLI also reports its host stage times with --verbose)
         fd2, opath = tempfile.mkstemp(prefix="scores_", suffix=".txt")
         os.close(fd2)
+        f2f_runs, stages = [], None
         try:
-            t0 = time.perf_counter()
-            subprocess.run([str(binary), "--inputfile", path, "--outputfile", opath], capture_output=True,
-                           text=True, check=True)
-            f2f = time.perf_counter() - t0
+            for _ in range(3):
+                cmd = [str(binary), "--inputfile", path, "--outputfile", opath]
+                if args.impl == "cli":
+                    cmd.append("--verbose")
+                t0 = time.perf_counter()
+                out2 = subprocess.run(cmd, capture_output=True, text=True, check=True).stdout
+                f2f_runs.append(time.perf_counter() - t0)
+                m2 = re.search(r"Host stages: engine start-up ([0-9.e+-]+)s, parse ([0-9.e+-]+)s, "
+                               r"format\+write ([0-9.e+-]+)s", out2)
+                if m2:
+                    stages = {"engine_start_s": float(m2.group(1)), "parse_s": float(m2.group(2)),
+                              "format_write_s": float(m2.group(3))}
+            f2f = statistics.median(f2f_runs)
             out_bytes = os.path.getsize(opath)
         finally:
             os.unlink(opath)
@@ -255,9 +266,11 @@ def run_binary(args, cfg):
                                 "parsing excluded), whole batch at once; median over the steps",
                       "step_seconds": [round(v[0], 4) for v in vals],
                       "file_to_file": {"wall_s": round(f2f, 3), "gcups": round(batch.cells() / f2f / 1e9, 3),
+                                       "runs_s": [round(x, 3) for x in f2f_runs], "last_run_stages": stages,
                                        "input_bytes": in_bytes,
                                        "output_bytes": out_bytes,
-                                       "command": "--inputfile records --outputfile scores (default batch sizes)"}}),
+                                       "command": "--inputfile records --outputfile scores (default batch sizes); "
+                                                  "median of 3"}}),
           flush=True)
 
 
