@@ -132,6 +132,10 @@ double oracle_pair_log10_gcp(const uint8_t* read, const uint8_t* bq, const uint8
         const float alpha_f = 1.0f - (delta_f + sigma_f);
         const double delta = delta_f, sigma = sigma_f, alpha = alpha_f;
         const int x = oracle_encode_base(read[r]);
+        /* emission by haplotype code for this read position */
+        double lamtab[5];
+        for (int hh = 0; hh < 5; ++hh)
+            lamtab[hh] = (x == 4 || hh == 4 || x == hh) ? (double)lam_match : (double)lam_mis;
 
         Mc[0] = 0.0; Ic[0] = 0.0; Dc[0] = 0.0;
         for (int k = 0; k < nb; ++k) {
@@ -149,8 +153,7 @@ double oracle_pair_log10_gcp(const uint8_t* read, const uint8_t* bq, const uint8
             double bmax = 0.0;
             if (fp == 1.0) { /* the block keeps its exponent: no scaling inside */
                 for (int c = c0; c <= c1; ++c) {
-                    const int h = hcode[c - 1];
-                    const double lam = (x == 4 || h == 4 || x == h) ? (double)lam_match : (double)lam_mis;
+                    const double lam = lamtab[hcode[c - 1]];
                     const double m = lam * (alpha * mdiag + beta * (idiag + ddiag));
                     const double i = delta * Mp[c] + eps * Ip[c];
                     const double d = sigma * mleft + eps * dleft;
@@ -163,8 +166,7 @@ double oracle_pair_log10_gcp(const uint8_t* read, const uint8_t* bq, const uint8
                 }
             } else {
                 for (int c = c0; c <= c1; ++c) {
-                    const int h = hcode[c - 1];
-                    const double lam = (x == 4 || h == 4 || x == h) ? (double)lam_match : (double)lam_mis;
+                    const double lam = lamtab[hcode[c - 1]];
                     const double mup = Mp[c] * fp, iup = Ip[c] * fp;
                     const double m = lam * (alpha * mdiag + beta * (idiag + ddiag));
                     const double i = delta * mup + eps * iup;
