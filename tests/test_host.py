@@ -285,3 +285,46 @@ def test_reader_reports_a_missing_file(tmp_path):
     with pytest.raises(g.PairHMMError) as e:
         g.RecordFileReader(tmp_path / "none.txt")
     assert "could not open" in str(e.value)
+
+
+def _random_record_text(seed: int, target_bytes: int) -> str:
+    """Well-formed records of random shape: R and H from 0, read lengths 1..300,
+    any printable quality characters, bases with N, lowercase and other letters."""
+    rng = np.random.default_rng(seed)
+    letters = np.frombuffer(b"ACGTACGTACGTNacgtRYX", dtype=np.uint8)
+    out, size = [], 0
+    while size < target_bytes:
+        R, H = int(rng.integers(0, 9)), int(rng.integers(0, 6))
+        lines = [f"{R} {H}"]
+        for _ in range(R):
+            L = int(rng.integers(1, 301))
+            bases = letters[rng.integers(0, len(letters), L)].tobytes().decode()
+            quals = [rng.integers(33, 127, L).astype(np.uint8).tobytes().decode() for _ in range(4)]
+            lines.append(" ".join([bases] + quals))
+        for _ in range(H):
+            lines.append(letters[rng.integers(0, len(letters), int(rng.integers(1, 500)))].tobytes().decode())
+        block = "\n".join(lines) + "\n"
+        out.append(block)
+        size += len(block)
+    return "".join(out)
+
+
+@pytest.mark.parametrize("seed,size", [(1, 20_000), (2, 200_000), (3, 2_600_000)])
+def test_parser_random_records_match_restatement(seed, size):
+    """The multi-threaded parser against the plain-Python restatement of the
+    reference's parser rules, on one thread and on several."""
+    text = _random_record_text(seed, size)
+    want = formats.to_soa(formats.parse_text(text))
+    try:
+        for threads in (1, 6):
+            g.set_host_threads(threads)
+            b = g.parse_records(text).batch
+            for k in ("reads_per_record", "haps_per_record", "read_offsets", "read_lengths", "hap_offsets",
+                      "hap_lengths"):
+                np.testing.assert_array_equal(np.asarray(getattr(b, k)), getattr(want, k), err_msg=f"{k} x{threads}")
+            n = len(want.read_bases)
+            for k in ("read_bases", "base_quals", "ins_quals", "del_quals", "gcp_quals"):
+                np.testing.assert_array_equal(np.asarray(getattr(b, k))[:n], getattr(want, k), err_msg=f"{k} x{threads}")
+            np.testing.assert_array_equal(np.asarray(b.hap_bases)[:len(want.hap_bases)], want.hap_bases)
+    finally:
+        g.set_host_threads(0)
