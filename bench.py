@@ -14,6 +14,15 @@ pass, and the download of the scores.
   roofline  11 FP32 FLOP per DP cell / time of the FP32 wavefront launches,
           against an FFMA peak measured on the same GPU in the same run
 
+Beside the headline line (single GPU only): the precision-stress and
+long-read configurations at their stated sizes (`stress`, `long`: device
+GCUPS, stage split, FP64 fractions, error against the FP64 oracle on a
+sample), the plain per-launch FP32 form on the same batch (`plain`,
+`vs_plain`), the reference's own gpuPairHMM binary built for sm_100a on the
+same batch as record text (`reference_gpu`, `vs_reference_gpu`, both by the
+binary's batch clock: upload, kernels, download), and the streaming service
+(`serving`: 60 s at 2,000 regions/s, then a sweep of higher rates).
+
 Multi-GPU (torchrun): each rank runs its own replica on its own batch (weak
 scaling, no data-path collective); times are the max over ranks.
 
@@ -60,9 +69,15 @@ def parse_args():
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU baseline sample size (seconds of work)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--accuracy-pairs", type=int, default=3000)
-    ap.add_argument("--serving-seconds", type=float, default=10.0,
-                    help="length of the streaming-service run (0 = skip); the full configuration is 60")
+    ap.add_argument("--serving-seconds", type=float, default=60.0,
+                    help="length of the streaming-service run at --serving-rate (0 = skip)")
     ap.add_argument("--serving-rate", type=float, default=2000.0, help="region arrivals per second")
+    ap.add_argument("--sweep-rates", default="8000,20000,40000,80000",
+                    help="further arrival rates of the serving sweep (comma separated, '' = none); "
+                         "stops at the first rate whose p99 exceeds 1 s")
+    ap.add_argument("--sweep-seconds", type=float, default=10.0)
+    ap.add_argument("--no-extra-configs", action="store_true",
+                    help="skip the precision-stress / long-read blocks, the plain form and the reference binary")
     return ap.parse_args()
 
 
@@ -315,64 +330,191 @@ def percentile(xs, q):
     return float(np.percentile(np.asarray(xs, dtype=np.float64), q)) if len(xs) else None
 
 
-def run_serving(args, local_rank):
-    """Streaming service: regions arrive as a Poisson stream (the uneven-length
-    region shapes, 5% long-read shapes) and are submitted to the engine's
-    continuous-batching queue as they arrive; each region's latency is from
-    submission to results ready on the host.  Beside it, the same stream through
-    one blocking plain-FP32 call per region in arrival order (latency from
-    arrival, so it includes waiting behind earlier regions)."""
-    import gpupairhmm_b200 as g
-    from gpupairhmm_b200 import synth
-    stream = [(t, r.contiguous()) for t, r in synth.stream_regions(seed=4, rate=args.serving_rate,
-                                                                    seconds=args.serving_seconds)]
-    cells = sum(r.cells() for _, r in stream)
-    pairs = sum(r.num_pairs for _, r in stream)
-    out = {"regions": len(stream), "rate_per_s": args.serving_rate, "seconds": args.serving_seconds,
-           "pairs": pairs, "cells": cells, "long_region_fraction": 0.05}
-
-    # continuous batching
-    eng = g.Engine(device=local_rank)
-    warm = [eng.submit(r) for _, r in stream[:200]]  # warm the queue's engines (a burst of both kinds)
-    for tk, (_, r) in zip(warm, stream[:200]):
-        eng.drain(tk, r.num_pairs)
+def _serve_stream(eng, pool, times, picks, cells_of):
+    """Submit pool regions at the given arrival times (busy wait), then collect.
+    Latency of a region = (submission - arrival) + the engine's submit-to-done
+    time, so a submit loop that falls behind shows up in it."""
     t0 = time.perf_counter()
     tickets = []
-    for t_arr, r in stream:
+    for t_arr, i in zip(times, picks):
         while time.perf_counter() - t0 < t_arr:
             pass
-        tickets.append((eng.submit(r), time.perf_counter() - t0, r.num_pairs))
+        t_sub = time.perf_counter() - t0
+        tickets.append((eng.submit(pool[i]), t_sub, t_sub - t_arr, pool[i].num_pairs))
     lat, done = [], []
-    for tk, t_sub, n in tickets:
+    for tk, t_sub, late, n in tickets:
         while not eng.poll(tk):
             time.sleep(0.0002)
         ms = eng.latency_ms(tk)
         eng.drain(tk, n)
-        lat.append(ms)
+        lat.append(late * 1e3 + ms)
         done.append(t_sub + ms / 1e3)
-    span = max(done)
-    eng.close()
-    out["continuous_batching"] = {"p50_ms": round(percentile(lat, 50), 3), "p99_ms": round(percentile(lat, 99), 3),
-                                  "max_ms": round(max(lat), 3), "gcups": round(cells / span / 1e9, 3),
-                                  "span_s": round(span, 3)}
+    span = max(done) if done else 1e-9
+    cells = sum(cells_of[i] for i in picks)
+    return {"regions": len(times), "p50_ms": round(percentile(lat, 50), 3), "p99_ms": round(percentile(lat, 99), 3),
+            "max_ms": round(max(lat), 3), "gcups": round(cells / span / 1e9, 3), "span_s": round(span, 3),
+            "offered_gcups": round(cells / max(float(times[-1]), 1e-9) / 1e9, 3) if len(times) else 0.0}
 
-    # one region per blocking call, plain FP32 form
+
+def run_serving(args, local_rank):
+    """Streaming service: regions arrive as a Poisson stream (the uneven-length
+    region shapes, 5% long-read shapes) and are submitted to the engine's
+    continuous-batching queue as they arrive.  Region shapes are drawn from a
+    pool of 24,000 regions generated ahead of time (the generator is far slower
+    than the arrival rates).  First the configured rate for the configured
+    length, then a sweep of higher rates until p99 exceeds 1 s.  Beside it, the
+    first 10 s of the configured stream through one blocking plain-FP32 call
+    per region in arrival order (latency from arrival)."""
+    import gpupairhmm_b200 as g
+    from gpupairhmm_b200 import synth
+    pool = synth.region_pool(seed=4, regions=24000, long_frac=0.05)
+    cells_of = [r.cells() for r in pool]
+    times, picks = synth.poisson_arrivals(5, args.serving_rate, args.serving_seconds, len(pool))
+    out = {"rate_per_s": args.serving_rate, "seconds": args.serving_seconds, "long_region_fraction": 0.05,
+           "pool": "24,000 regions drawn ahead of time (seed 4), picked uniformly per arrival",
+           "latency": "arrival to scores on the host (submission delay + submit-to-done)"}
+
+    eng = g.Engine(device=local_rank)
+    warm = [eng.submit(r) for r in pool[:300]]  # warm the queue's engines (a burst of both kinds)
+    for tk, r in zip(warm, pool[:300]):
+        eng.drain(tk, r.num_pairs)
+    out["continuous_batching"] = _serve_stream(eng, pool, times, picks, cells_of)
+    sweep = []
+    for k, rate in enumerate(float(x) for x in args.sweep_rates.split(",") if x.strip()):
+        tt, pp = synth.poisson_arrivals(6 + k, rate, args.sweep_seconds, len(pool))
+        point = dict(rate_per_s=rate, seconds=args.sweep_seconds, **_serve_stream(eng, pool, tt, pp, cells_of))
+        sweep.append(point)
+        if point["p99_ms"] > 1000.0:
+            break
+    out["sweep"] = sweep
+    out["admission"] = eng.serving_stats()
+    eng.close()
+
+    # one region per blocking call, plain FP32 form, first 10 s of the stream
     pe = g.Engine(device=local_rank, mode=g.MODE_PLAIN)
-    for _, r in stream[:200]:
+    for r in pool[:200]:
         pe.compute(r)
+    n10 = int(np.searchsorted(times, min(10.0, args.serving_seconds), side="right"))
     lat = []
     t0 = time.perf_counter()
-    for t_arr, r in stream:
+    for t_arr, i in zip(times[:n10], picks[:n10]):
         while time.perf_counter() - t0 < t_arr:
             pass
-        pe.compute(r)
+        pe.compute(pool[i])
         lat.append((time.perf_counter() - t0 - t_arr) * 1e3)
     span = time.perf_counter() - t0
     pe.close()
-    out["plain_per_region"] = {"p50_ms": round(percentile(lat, 50), 3), "p99_ms": round(percentile(lat, 99), 3),
-                               "max_ms": round(max(lat), 3), "gcups": round(cells / span / 1e9, 3),
+    cells10 = sum(cells_of[i] for i in picks[:n10])
+    out["plain_per_region"] = {"regions": n10, "seconds_of_stream": min(10.0, args.serving_seconds),
+                               "p50_ms": round(percentile(lat, 50), 3), "p99_ms": round(percentile(lat, 99), 3),
+                               "max_ms": round(max(lat), 3), "gcups": round(cells10 / span / 1e9, 3),
                                "span_s": round(span, 3)}
     return out
+
+
+def region_accuracy(batch, scores, regions, seed):
+    """|log10 difference| against the FP64 oracle on every pair of `regions`
+    randomly chosen records."""
+    import oracle
+    from gpupairhmm_b200 import replicas, synth
+    rng = np.random.default_rng(seed)
+    pick = np.sort(rng.choice(batch.num_records, size=min(batch.num_records, regions), replace=False))
+    po = replicas.pair_offsets(batch)
+    sub = synth.concat([batch.select_records(int(r), int(r) + 1) for r in pick])
+    want = oracle.batch_log10(sub)
+    got = np.concatenate([scores[po[r]:po[r + 1]] for r in pick]).astype(np.float64)
+    err = np.abs(got - want)
+    rel = err / np.maximum(np.abs(want), 1e-30)
+    return {"sample_regions": int(len(pick)), "sample_pairs": int(len(want)), "sample_cells": int(sub.cells()),
+            "max_abs_log10": float(err.max()), "mean_abs_log10": float(err.mean()),
+            "max_rel_log10": float(rel.max()), "min_log10": float(want.min()),
+            "within_1e-5_rel": bool(np.all(err <= 1e-5 * np.abs(want) + 1e-6))}
+
+
+def run_config(name, batch, desc, steps, warmup, local_rank, acc_regions):
+    """One configuration at its stated size through a one-pass engine (inputs
+    page-locked; device time after the upload), its FP32-only result from the
+    plain form (how many pairs the FP32 recurrence alone loses), and the error
+    against the FP64 oracle on a sample of regions."""
+    import torch
+    import gpupairhmm_b200 as g
+    pinned = batch.pin()
+    scores = torch.empty(batch.num_pairs, dtype=torch.float32).pin_memory().numpy()
+    eng = g.Engine(device=local_rank, pipeline_chunks=1)
+    for _ in range(warmup):
+        eng.compute(pinned, out=scores)
+    dev = fp32 = fp64 = prep = 0.0
+    for _ in range(steps):
+        eng.compute(pinned, out=scores)
+        st = eng.stats()
+        dev += st.device_ms
+        fp32 += st.fp32_ms
+        fp64 += st.fp64_ms
+        prep += st.prep_ms
+    eng.close()
+    cells = batch.cells()
+    out = {"workload": desc, "pairs": batch.num_pairs, "cells": cells, "steps": steps,
+           "gcups": round(cells * steps / (dev / 1e3) / 1e9, 3), "ms_per_step": round(dev / steps, 3),
+           "stage_ms_per_step": {"prep": round(prep / steps, 3), "fp32": round(fp32 / steps, 3),
+                                 "fp64": round(fp64 / steps, 3)},
+           "fp64_fraction": round(st.rescued / batch.num_pairs, 5),
+           "fp64_extended_fraction": round(st.rescued_ext / batch.num_pairs, 6),
+           "fp64_pairs": int(st.rescued), "fp64_extended_pairs": int(st.rescued_ext)}
+    pe = g.Engine(device=local_rank, mode=g.MODE_PLAIN, pipeline_chunks=1)
+    fp32_only = pe.compute(pinned)
+    pe.close()
+    out["fp32_only_nonfinite_fraction"] = round(float(np.mean(~np.isfinite(fp32_only))), 5)
+    out["accuracy"] = region_accuracy(batch, scores, acc_regions, seed=17)
+    return out
+
+
+def run_plain(batch_pinned, cells, steps, warmup, local_rank):
+    """The plain per-launch FP32 form on the same batch: the reference's tile
+    table and launch shape (one launch per length partition), FP32 only, device
+    time with inputs resident."""
+    import gpupairhmm_b200 as g
+    pe = g.Engine(device=local_rank, mode=g.MODE_PLAIN, pipeline_chunks=1)
+    for _ in range(warmup):
+        pe.compute(batch_pinned)
+    dev = 0.0
+    for _ in range(steps):
+        pe.compute(batch_pinned)
+        dev += pe.stats().device_ms
+    pe.close()
+    return {"gcups": round(cells * steps / (dev / 1e3) / 1e9, 3), "ms_per_step": round(dev / steps, 3),
+            "steps": steps, "form": "reference tile table (tuningconfigs.hpp:33-57), one non-persistent launch "
+                                    "per partition, this engine's FP32 cell, no FP64 pass"}
+
+
+def run_reference_binary(batch, steps):
+    """The reference's gpuPairHMM, built from its sources for sm_100a into
+    oracle/_ref, on the same batch as a record file; GCUPS by its own batch
+    clock (upload, kernels, download), median over the runs."""
+    import re
+    from gpupairhmm_b200 import synth
+    binary = ROOT / "oracle" / "_ref" / "gpuPairHMM"
+    if not binary.exists():
+        return {"unavailable": "oracle/_ref/gpuPairHMM not built"}
+    fd, path = tempfile.mkstemp(prefix="records_", suffix=".txt")
+    os.close(fd)
+    try:
+        Path(path).write_text(synth.to_text(batch))
+        runs = []
+        for _ in range(steps + 1):
+            out = subprocess.run([str(binary), "--inputfile", path, "--outputfile", "/dev/null",
+                                  "--fileBatchsize", "0", "--transferBatchsize", "0"],
+                                 capture_output=True, text=True, timeout=600).stdout
+            m = re.search(r"Batch processing time: ([0-9.e+-]+)s \(([0-9.e+-]+) GCUPS\)", out)
+            if not m:
+                return {"unavailable": "no batch time in the binary's output"}
+            runs.append(float(m.group(1)))
+    finally:
+        os.unlink(path)
+    sec = statistics.median(runs[1:])
+    return {"gcups": round(batch.cells() / sec / 1e9, 3), "batch_seconds": [round(x, 4) for x in runs[1:]],
+            "timing": "the binary's printed batch time (upload, kernels, download; file parse excluded), "
+                      "median of the runs after one warm-up, no profiler attached",
+            "build": "oracle/Makefile from the reference's sources, sm_100a, generic tuning table"}
 
 
 def run_ours(args, cfg, rank, world, local_rank):
@@ -413,7 +555,7 @@ def run_ours(args, cfg, rank, world, local_rank):
     sampler.start()
     time.sleep(0.25)
     dev_ms = fp32_ms = prep_ms = fp64_ms = 0.0
-    launches = h2d = d2h = rescued = 0
+    launches = fp32_launches = h2d = d2h = rescued = rescued_ext = 0
     for _ in range(args.steps):
         engine_dev.compute(pinned, out=scores)
         st = engine_dev.stats()
@@ -422,7 +564,9 @@ def run_ours(args, cfg, rank, world, local_rank):
         prep_ms += st.prep_ms
         fp64_ms += st.fp64_ms
         launches += st.launches
+        fp32_launches += st.fp32_launches
         rescued = st.rescued
+        rescued_ext = st.rescued_ext
     torch.cuda.synchronize()
     if dist:
         dist.barrier()
@@ -452,14 +596,14 @@ def run_ours(args, cfg, rank, world, local_rank):
         e2e = total_cells / wall / 1e9
         achieved = FLOPS_PER_CELL * cells * args.steps / fp32_s / 1e12
         tpc = traffic_per_cell()
-        n_fp32_launches = max(1, launches // max(1, args.steps) - 7)
+        n_fp32_launches = max(1, fp32_launches // max(1, args.steps))
         rng = np.random.default_rng(99)
         line = {
             "metric": METRIC, "value": round(value, 3), "unit": "GCUPS", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(dev_s / args.steps * 1e3, 3), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "fp32", "data": "synthetic",
             "config": dict(cfg, pairs=batch.num_pairs, cells=cells, rescued_fp64=rescued,
-                           parallelism=f"replicas{world}"),
+                           rescued_fp64_extended=rescued_ext, parallelism=f"replicas{world}"),
             "e2e": {"value": round(e2e, 3), "unit": "GCUPS", "h2d_bytes_per_step": h2d // args.steps,
                     "d2h_bytes_per_step": d2h // args.steps, "ms_per_step": round(wall / args.steps * 1e3, 3)},
             "gpu_launches": int(launches),
@@ -477,11 +621,31 @@ def run_ours(args, cfg, rank, world, local_rank):
                                                "fp64": round(fp64_ms / args.steps, 3)}},
             "clocks": clocks,
         }
-        # the streaming-service run goes first: after the OpenMP oracle has run in
-        # this process (accuracy sample, CPU baseline) the serving threads saw
-        # periodic host stalls of several hundred ms
+        engine.close()
+        engine_dev.close()
+        extras = world == 1 and not args.no_extra_configs
+        if extras:
+            # the 1.5x target's denominator and the reference's own kernels, same batch
+            line["plain"] = run_plain(pinned, cells, 3, 2, local_rank)
+            line["vs_plain"] = round(value / line["plain"]["gcups"], 4)
+            ref = run_reference_binary(batch, 3)
+            line["reference_gpu"] = ref
+            line["vs_reference_gpu"] = round(e2e / ref["gcups"], 4) if "gcups" in ref else None
+        # the streaming-service run goes before anything that runs the OpenMP oracle
+        # in this process (accuracy samples, CPU baseline): after it, the serving
+        # threads saw periodic host stalls of several hundred ms
         if world == 1 and args.serving_seconds > 0:
             line["serving"] = run_serving(args, local_rank)
+        if extras:
+            line["stress"] = run_config(
+                "stress", synth.config2(seed=2, regions=5000),
+                "precision stress: 5,000 regions x R=64 x H=8, reads 250 bp, haplotypes 600 bp, half of the "
+                "reads unrelated, base quality U{35..41}, ins/del 40, gcp 10", 3, 2, local_rank, 40)
+            line["long"] = run_config(
+                "long", synth.config3(seed=3, regions=2000),
+                "long reads: 2,000 regions x R=16 x H=4, reads U{1000..2000}, haplotypes U{2000..5000} with "
+                "1-50 bp indels, base quality U{5..40}, ins/del U{30..45} per position, gcp 10", 3, 2,
+                local_rank, 16)
         if world == 1:
             line["host_io"] = host_io(batch)
         line["accuracy"] = accuracy(batch, scores, args.accuracy_pairs, rng)
@@ -491,8 +655,9 @@ def run_ours(args, cfg, rank, world, local_rank):
             line["cpu_baseline"] = {"value": round(gc, 4), "unit": "GCUPS", "cores": os.cpu_count() or 1,
                                     "kind": "port", "sample": desc + "; FP64 oracle, OpenMP over pairs"}
         print(json.dumps(line), flush=True)
-    engine.close()
-    engine_dev.close()
+    else:
+        engine.close()
+        engine_dev.close()
     if dist:
         dist.barrier()
         dist.destroy_process_group()

@@ -89,6 +89,20 @@ class _Stats(ctypes.Structure):
         ("launches", ctypes.c_int64),
         ("h2d_bytes", ctypes.c_int64),
         ("d2h_bytes", ctypes.c_int64),
+        ("rescued_ext", ctypes.c_int64),
+        ("fp32_launches", ctypes.c_int64),
+    ]
+
+
+class _ServingStats(ctypes.Structure):
+    _fields_ = [
+        ("regions", ctypes.c_int64),
+        ("batches", ctypes.c_int64),
+        ("max_batch_regions", ctypes.c_int64),
+        ("max_batch_bytes", ctypes.c_int64),
+        ("budget_per_slot", ctypes.c_int64),
+        ("slots", ctypes.c_int32),
+        ("max_in_flight", ctypes.c_int32),
     ]
 
 
@@ -105,6 +119,7 @@ _SIGNATURES = {
     "pairhmm_poll": (ctypes.c_int, [_P, ctypes.c_uint64, _P]),
     "pairhmm_drain": (ctypes.c_int, [_P, ctypes.c_uint64, _P, ctypes.c_int64, ctypes.c_int32]),
     "pairhmm_region_latency_ms": (ctypes.c_int, [_P, ctypes.c_uint64, _P]),
+    "pairhmm_serving_stats": (ctypes.c_int, [_P, _P]),
     "pairhmm_set_tile_table": (ctypes.c_int, [_P, _P, _P, _P, _P, ctypes.c_int32]),
     "pairhmm_get_tile_table": (ctypes.c_int, [_P, _P, _P, _P, _P, ctypes.c_int32, _P]),
     "pairhmm_probe_fp32_peak": (ctypes.c_int, [ctypes.c_int32, ctypes.c_int32, _P]),
@@ -255,6 +270,8 @@ class Stats:
     launches: int
     h2d_bytes: int
     d2h_bytes: int
+    rescued_ext: int = 0
+    fp32_launches: int = 0
 
 
 class Engine:
@@ -321,7 +338,8 @@ class Engine:
         st = _Stats()
         _check(lib().pairhmm_get_stats(self._h, ctypes.byref(st)), self._h)
         return Stats(st.pairs, st.cells, st.rescued, st.multi_tile_pairs, st.device_ms, st.total_ms, st.prep_ms,
-                     st.fp32_ms, st.fp64_ms, st.launches, st.h2d_bytes, st.d2h_bytes)
+                     st.fp32_ms, st.fp64_ms, st.launches, st.h2d_bytes, st.d2h_bytes, st.rescued_ext,
+                     st.fp32_launches)
 
     # ------------------------------------------------------------ serving
     def submit(self, region: Batch) -> int:
@@ -345,6 +363,13 @@ class Engine:
         out = np.empty(max(num_scores, 1), dtype=np.float32)
         _check(lib().pairhmm_drain(self._h, ticket, _ptr(out), num_scores, timeout_ms), self._h)
         return out[:num_scores]
+
+    def serving_stats(self) -> dict:
+        """Admission record of the serving queue (batches, most regions and
+        bytes in one batch, slot budget, most batches in flight)."""
+        st = _ServingStats()
+        _check(lib().pairhmm_serving_stats(self._h, ctypes.byref(st)), self._h)
+        return {name: int(getattr(st, name)) for name, _ in _ServingStats._fields_}
 
     # ------------------------------------------------------------ tuning
     def tile_table(self) -> list[tuple[int, int, int, int]]:

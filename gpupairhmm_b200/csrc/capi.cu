@@ -1,6 +1,7 @@
 // extern "C" boundary: no C++ exceptions or types cross it.
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <new>
 
 #include "engine.hpp"
@@ -24,30 +25,51 @@ thread_local std::string t_records_error;
 struct pairhmm_engine {
     std::unique_ptr<phmm::Engine> engine;
     std::unique_ptr<phmm::ServingQueue> serving;
+    std::mutex serving_mu;  // creation of the serving queue; its calls may overlap
+    std::mutex error_mu;    // error text: serving calls may come from several threads
     std::string error;
 };
 
 namespace {
+
+void set_error(pairhmm_engine* h, std::string msg) {
+    if (!h) return;
+    std::lock_guard<std::mutex> lk(h->error_mu);
+    h->error = std::move(msg);
+}
 
 template <class F>
 pairhmm_status_t guarded(pairhmm_engine* h, F&& f) {
     try {
         return f();
     } catch (const std::bad_alloc&) {
-        if (h) h->error = "host allocation failed";
+        set_error(h, "host allocation failed");
         return PAIRHMM_ERR_OUT_OF_MEMORY;
     } catch (const std::exception& e) {
-        if (h) h->error = e.what();
+        set_error(h, e.what());
         return PAIRHMM_ERR_CUDA;
     } catch (...) {
-        if (h) h->error = "unknown exception";
+        set_error(h, "unknown exception");
         return PAIRHMM_ERR_CUDA;
     }
 }
 
+// the serving queue of an engine, created on first use
+phmm::ServingQueue* serving_of(pairhmm_engine* h, bool create) {
+    std::lock_guard<std::mutex> lk(h->serving_mu);
+    if (!h->serving && create) h->serving = std::make_unique<phmm::ServingQueue>(*h->engine);
+    return h->serving.get();
+}
+
+pairhmm_status_t serving_result(pairhmm_engine* h, phmm::ServingQueue* q, pairhmm_status_t s) {
+    if (s != PAIRHMM_OK) {
+        set_error(h, q ? q->last_error() : std::string("no region was submitted to this engine"));
+    }
+    return s;
+}
+
 pairhmm_status_t finish(pairhmm_engine* h, pairhmm_status_t s) {
-    if (s != PAIRHMM_OK) h->error = h->engine->last_error();
-    else h->error.clear();
+    set_error(h, s != PAIRHMM_OK ? h->engine->last_error() : std::string());
     return s;
 }
 
@@ -121,20 +143,16 @@ pairhmm_status_t pairhmm_get_stats(pairhmm_engine_t* h, pairhmm_stats_t* stats) 
 pairhmm_status_t pairhmm_submit(pairhmm_engine_t* h, const pairhmm_batch_t* region, uint64_t* ticket) {
     if (!h || !region || !ticket) return PAIRHMM_ERR_INVALID_ARGUMENT;
     return guarded(h, [&] {
-        if (!h->serving) h->serving = std::make_unique<phmm::ServingQueue>(*h->engine);
-        pairhmm_status_t s = h->serving->submit(*region, ticket);
-        if (s != PAIRHMM_OK) h->error = h->serving->last_error();
-        return s;
+        phmm::ServingQueue* q = serving_of(h, true);
+        return serving_result(h, q, q->submit(*region, ticket));
     });
 }
 
 pairhmm_status_t pairhmm_poll(pairhmm_engine_t* h, uint64_t ticket, int32_t* done) {
     if (!h || !done) return PAIRHMM_ERR_INVALID_ARGUMENT;
     return guarded(h, [&] {
-        if (!h->serving) return PAIRHMM_ERR_NOT_FOUND;
-        pairhmm_status_t s = h->serving->poll(ticket, done);
-        if (s != PAIRHMM_OK) h->error = h->serving->last_error();
-        return s;
+        phmm::ServingQueue* q = serving_of(h, false);
+        return serving_result(h, q, q ? q->poll(ticket, done) : PAIRHMM_ERR_NOT_FOUND);
     });
 }
 
@@ -142,21 +160,25 @@ pairhmm_status_t pairhmm_drain(pairhmm_engine_t* h, uint64_t ticket, float* scor
                                int32_t timeout_ms) {
     if (!h || (!scores && num_scores > 0)) return PAIRHMM_ERR_INVALID_ARGUMENT;
     return guarded(h, [&] {
-        if (!h->serving) return PAIRHMM_ERR_NOT_FOUND;
-        pairhmm_status_t s = h->serving->drain(ticket, scores, num_scores, timeout_ms);
-        if (s != PAIRHMM_OK) h->error = h->serving->last_error();
-        return s;
+        phmm::ServingQueue* q = serving_of(h, false);
+        return serving_result(h, q, q ? q->drain(ticket, scores, num_scores, timeout_ms) : PAIRHMM_ERR_NOT_FOUND);
     });
 }
 
 pairhmm_status_t pairhmm_region_latency_ms(pairhmm_engine_t* h, uint64_t ticket, double* ms) {
     if (!h || !ms) return PAIRHMM_ERR_INVALID_ARGUMENT;
     return guarded(h, [&] {
-        if (!h->serving) return PAIRHMM_ERR_NOT_FOUND;
-        pairhmm_status_t s = h->serving->latency(ticket, ms);
-        if (s != PAIRHMM_OK) h->error = h->serving->last_error();
-        return s;
+        phmm::ServingQueue* q = serving_of(h, false);
+        return serving_result(h, q, q ? q->latency(ticket, ms) : PAIRHMM_ERR_NOT_FOUND);
     });
+}
+
+pairhmm_status_t pairhmm_serving_stats(pairhmm_engine_t* h, pairhmm_serving_stats_t* stats) {
+    if (!h || !stats) return PAIRHMM_ERR_INVALID_ARGUMENT;
+    *stats = pairhmm_serving_stats_t{};
+    phmm::ServingQueue* q = serving_of(h, false);
+    if (q) q->stats(stats);
+    return PAIRHMM_OK;
 }
 
 const char* pairhmm_status_string(pairhmm_status_t s) {
@@ -175,7 +197,14 @@ const char* pairhmm_status_string(pairhmm_status_t s) {
     return "unknown status";
 }
 
-const char* pairhmm_last_error(const pairhmm_engine_t* h) { return h ? h->error.c_str() : ""; }
+const char* pairhmm_last_error(const pairhmm_engine_t* h) {
+    // a copy per calling thread: serving calls on other threads may replace the text
+    thread_local std::string copy;
+    if (!h) return "";
+    std::lock_guard<std::mutex> lk(const_cast<pairhmm_engine_t*>(h)->error_mu);
+    copy = h->error;
+    return copy.c_str();
+}
 
 pairhmm_status_t pairhmm_batch_counts(const pairhmm_batch_t* batch, int64_t* pairs, int64_t* cells) {
     if (!batch) return PAIRHMM_ERR_INVALID_ARGUMENT;

@@ -61,6 +61,15 @@ struct Item {
 };
 static_assert(sizeof(Item) == 32, "Item must be 32 bytes");
 
+// Where the FP64 pass's scaled tier sends the pairs beyond its range: the
+// extended tier's class lists (same class offsets as the rescue lists) and
+// their counts.
+struct ExtList {
+    Task* base;
+    const long long* off;        // [kFp64Classes]
+    unsigned long long* count;   // [kFp64Classes]
+};
+
 struct DevView;
 __device__ __forceinline__ void append_rescue(const DevView& v, int cls, const Task& t);
 

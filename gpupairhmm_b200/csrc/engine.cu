@@ -6,7 +6,8 @@
 //   bin_count, hist_scan,
 //   schedule, bin_scatter       sorted work list + per-bucket task ranges
 //   fp32_bucket_kernel<G,R,MT>  one launch per non-empty length bucket
-//   fp64_rescue_kernel          pairs flagged by the FP32 pass
+//   fp64_rescue_kernel<scaled>  pairs flagged by the FP32 pass, in doubles
+//   fp64_rescue_kernel<ext>     the few beyond the scaled doubles' range
 // Compared with the reference executor (gpuworker.cuh:559-973) there is no
 // device-to-host synchronisation inside a batch: the host derives bucket sizes
 // from the record structure it already holds, and the kernels read their task
@@ -25,6 +26,15 @@ namespace phmm {
 namespace {
 
 constexpr int64_t kScratchBudget = int64_t(4) << 30;  // border scratch cap per batch
+
+// Device counters of a batch (one array, zeroed by the fill kernel): bucket
+// task counters, then per FP64 length class the scaled tier's list counts, the
+// extended tier's list counts, and the two tiers' task counters.
+constexpr int kCtrScaled = kMaxBuckets;
+constexpr int kCtrExt = kMaxBuckets + kFp64Classes;
+constexpr int kCtrTaskScaled = kMaxBuckets + 2 * kFp64Classes;
+constexpr int kCtrTaskExt = kMaxBuckets + 3 * kFp64Classes;
+constexpr int kCtrTotal = kMaxBuckets + 4 * kFp64Classes;
 
 std::vector<TileRule> engine_default_rules() {
     // Tile per read-length bucket for the persistent engine, measured on a B200
@@ -101,6 +111,7 @@ std::vector<DevBuf*> Engine::all_buffers() {
             &read_record_, &read_local_, &rec_haps_, &rec_hap_base_, &rec_pair_base_, &read_start_,
             &hap_start_, &read_pack_, &hap_code_, &hist_, &cursor_, &items_, &rescue_, &counters_,
             &sched_, &scores_, &scratch_, &lens_tmp_, &unit_read0_, &unit_read1_, &unit_bucket_, &rescue_off_,
+            &rescue_ext_, &rsort_,
             &in_gq_, &read_gcp_};
 }
 
@@ -173,7 +184,7 @@ pairhmm_status_t Engine::init() {
             b->stream = stream_;
         }
     }
-    PHMM_CUDA(cudaMallocHost(&host_hdr_, 64));
+    PHMM_CUDA(cudaMallocHost(&host_hdr_, 256));
     PHMM_CUDA(cudaEventCreate(&ev0_));
     PHMM_CUDA(cudaEventCreate(&ev1_));
     PHMM_CUDA(cudaEventCreate(&ev_prep_));
@@ -184,15 +195,18 @@ pairhmm_status_t Engine::init() {
         PHMM_CUDA(cudaFuncSetAttribute(c.kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c.smem_bytes));
     for (int c = 0; c < kFp64Classes; ++c)
         for (const bool gcp : {false, true})
-            PHMM_CUDA(cudaFuncSetAttribute(fp64_kernel(c, gcp), cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           (int)fp64_smem_bytes(c)));
+            for (const bool ext : {false, true})
+                PHMM_CUDA(cudaFuncSetAttribute(fp64_kernel(c, gcp, ext), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                               (int)fp64_smem_bytes(c, ext)));
 
     // probability table p(q) = float(10^(-q/10)) (gpuworker.cuh:473-486)
     float table[128];
     for (int i = 0; i < 128; ++i) table[i] = (float)std::pow(10.0, (-i) / 10.0);
     PHMM_CUDA(ph2pr_.ensure(sizeof(table)));
     PHMM_CUDA(cudaMemcpy(ph2pr_.ptr, table, sizeof(table), cudaMemcpyHostToDevice));
-    PHMM_CUDA(counters_.ensure(sizeof(unsigned long long) * (kMaxBuckets + 2 * kFp64Classes)));
+    PHMM_CUDA(counters_.ensure(sizeof(unsigned long long) * kCtrTotal));
+    // FP64 list sort: per-class histogram (uint32) then cursors (uint64)
+    PHMM_CUDA(rsort_.ensure((sizeof(unsigned int) + sizeof(unsigned long long)) * kFp64Classes * kRescueHBins));
     PHMM_CUDA(sched_.ensure(sizeof(Schedule)));
     ready_ = true;
     return upload_rules();
@@ -513,6 +527,7 @@ pairhmm_status_t Engine::ensure_buffers(const BatchIndex& x, bool host_inputs) {
     PHMM_CUDA(cursor_.ensure(8 * nbins));
     PHMM_CUDA(items_.ensure(sizeof(Item) * np));
     PHMM_CUDA(rescue_.ensure(sizeof(Task) * np));  // class lists laid out back to back
+    PHMM_CUDA(rescue_ext_.ensure(sizeof(Task) * np));  // the extended tier's, same offsets
     PHMM_CUDA(rescue_off_.ensure(sizeof(int64_t) * kFp64Classes));
     return PAIRHMM_OK;
 }
@@ -580,15 +595,17 @@ pairhmm_status_t Engine::enqueue_pipeline(const pairhmm_batch_t& in, const Batch
     pa.hap_code = hap_code_.as<uint8_t>();
     if (stage == 0) {
     launches_ = 0;
+    fp32_launches_ = 0;
     // zero the histogram and the work/rescue counters, pad the haplotype codes
     // (a kernel, not memset nodes: see launch_fill)
     {
-        uint8_t* const ptr[3] = {hap_code_.as<uint8_t>() + x.code_bytes, hist_.as<uint8_t>(),
-                                 counters_.as<uint8_t>()};
-        const long long bytes[3] = {kHapSlack, (long long)sizeof(unsigned int) * nb * (plain ? 1 : kHBins),
-                                    (long long)sizeof(unsigned long long) * (kMaxBuckets + 2 * kFp64Classes)};
-        const int value[3] = {4, 0, 0};
-        PHMM_CUDA(launch_fill(ptr, bytes, value, 3, s));
+        uint8_t* const ptr[4] = {hap_code_.as<uint8_t>() + x.code_bytes, hist_.as<uint8_t>(),
+                                 counters_.as<uint8_t>(), rsort_.as<uint8_t>()};
+        const long long bytes[4] = {kHapSlack, (long long)sizeof(unsigned int) * nb * (plain ? 1 : kHBins),
+                                    (long long)sizeof(unsigned long long) * kCtrTotal,
+                                    (long long)sizeof(unsigned int) * kFp64Classes * kRescueHBins};
+        const int value[4] = {4, 0, 0, 0};
+        PHMM_CUDA(launch_fill(ptr, bytes, value, 4, s));
         launches_ += 1;
     }
     PHMM_CUDA(launch_pack(pa, prep_grid, s));
@@ -629,10 +646,30 @@ pairhmm_status_t Engine::enqueue_pipeline(const pairhmm_batch_t& in, const Batch
     v.scores = d_scores;
     v.rescue_base = rescue_.as<Task>();
     v.rescue_off = rescue_off_.as<long long>();
-    v.rescue_count = counters + kMaxBuckets;
+    v.rescue_count = counters + kCtrScaled;
     v.rescue_enabled = (!plain && opts_.fp64_rescue) ? 1 : 0;
     v.ph2pr = ph2pr_.as<float>();
     v.read_gcp = pa.read_gcp;
+
+    // FP64 pass: first sort each class's list by haplotype length into the
+    // work-item buffer (free once the FP32 stage is done), same class offsets
+    Task* const fp64_lists = items_.as<Task>();
+    int64_t fp64_upper = 0;  // pairs the FP64 lists could hold
+    for (int c = 0; c < kFp64Classes; ++c) fp64_upper += x.class_pairs[c];
+    if (stage == 2 && fp64_upper > 0) {
+        const int64_t upper = fp64_upper;
+        RescueSortArgs ra{};
+        ra.in = rescue_.as<Task>();
+        ra.out = fp64_lists;
+        ra.off = rescue_off_.as<long long>();
+        ra.count = counters + kCtrScaled;
+        ra.hap_len = in.hap_lengths;
+        ra.hist = rsort_.as<unsigned int>();
+        ra.cursor = reinterpret_cast<unsigned long long*>(rsort_.as<unsigned int>() + kFp64Classes * kRescueHBins);
+        const int sort_grid = (int)std::max<int64_t>(1, std::min<int64_t>((upper + 255) / 256, 8 * (int64_t)num_sms_));
+        PHMM_CUDA(launch_rescue_sort(ra, sort_grid, s));
+        launches_ += 3;
+    }
 
     // engine form: the stage's launches go round-robin onto the side streams
     // (forked from s, joined back below); the plain form keeps one stream
@@ -661,25 +698,34 @@ pairhmm_status_t Engine::enqueue_pipeline(const pairhmm_batch_t& in, const Batch
             la.stream = next_stream();
             PHMM_CUDA(c->launch(la));
             ++launches_;
+            ++fp32_launches_;
         }
     } else {
-        // stage 2: FP64 pass over flagged pairs (FP32 underflow, or degenerate alpha);
-        // only the last class uses the border scratch
+        // stage 2: FP64 pass over flagged pairs (FP32 underflow, or degenerate alpha):
+        // per length class the scaled tier, then on the same stream the extended
+        // tier over the pairs the scaled tier handed on; only the last class uses
+        // the border scratch (the two tiers of a class run in turn, so they share it)
+        const ExtList ext{rescue_ext_.as<Task>(), rescue_off_.as<long long>(), counters + kCtrExt};
         for (int c = 0; c < kFp64Classes; ++c) {
             if (x.class_pairs[c] == 0) continue;
-            Fp64LaunchArgs fa{};
-            fa.view = v;
-            fa.cls = c;
-            fa.gcp = opts_.gcp != 0;
-            fa.items = rescue_.as<Task>() + x.class_start[c];
-            fa.count = counters + kMaxBuckets + c;
-            fa.counter = counters + kMaxBuckets + kFp64Classes + c;
-            fa.scratch = scratch_.ptr;
-            fa.rows = plan.rows;
-            fa.grid = plan.fp64_grid[c];
-            fa.stream = next_stream();
-            PHMM_CUDA(launch_fp64_rescue(fa));
-            ++launches_;
+            const cudaStream_t sc = next_stream();
+            for (const bool tier_ext : {false, true}) {
+                Fp64LaunchArgs fa{};
+                fa.view = v;
+                fa.cls = c;
+                fa.gcp = opts_.gcp != 0;
+                fa.ext = tier_ext;
+                fa.ext_list = ext;
+                fa.items = (tier_ext ? rescue_ext_.as<Task>() : fp64_lists) + x.class_start[c];
+                fa.count = counters + (tier_ext ? kCtrExt : kCtrScaled) + c;
+                fa.counter = counters + (tier_ext ? kCtrTaskExt : kCtrTaskScaled) + c;
+                fa.scratch = scratch_.ptr;
+                fa.rows = plan.rows;
+                fa.grid = tier_ext ? plan.fp64_ext_grid[c] : plan.fp64_grid[c];
+                fa.stream = sc;
+                PHMM_CUDA(launch_fp64_rescue(fa));
+                ++launches_;
+            }
         }
     }
     if (fork) {
@@ -725,16 +771,18 @@ Engine::Plan Engine::make_plan(const BatchIndex& x) const {
         p.persistent[b] = (!plain || grid < need_blocks) ? 1 : 0;
     }
     for (int c = 0; c < kFp64Classes; ++c) {
-        int64_t grid = persistent_grid(fp64_kernel(c, opts_.gcp != 0), fp64_smem_bytes(c));
-        const int64_t per_warp = (int64_t)fp64_scratch_bytes_per_row(c) * p.rows;
-        if (per_warp > 0) {
-            grid = std::min<int64_t>(grid, std::max<int64_t>(1, kScratchBudget / (per_warp * kWarpsPerBlock)));
-            scratch = std::max(scratch, grid * kWarpsPerBlock * per_warp);
+        for (const bool tier_ext : {false, true}) {
+            int64_t grid = persistent_grid(fp64_kernel(c, opts_.gcp != 0, tier_ext), fp64_smem_bytes(c, tier_ext));
+            const int64_t per_warp = (int64_t)fp64_scratch_bytes_per_row(c, tier_ext) * p.rows;
+            if (per_warp > 0) {
+                grid = std::min<int64_t>(grid, std::max<int64_t>(1, kScratchBudget / (per_warp * kWarpsPerBlock)));
+                scratch = std::max(scratch, grid * kWarpsPerBlock * per_warp);
+            }
+            // no more warps than flagged pairs could need
+            const int64_t need = (x.class_pairs[c] + fp64_per_warp(c) - 1) / fp64_per_warp(c);
+            grid = std::min<int64_t>(grid, std::max<int64_t>(1, (need + kWarpsPerBlock - 1) / kWarpsPerBlock));
+            (tier_ext ? p.fp64_ext_grid : p.fp64_grid)[c] = (int)grid;
         }
-        // no more warps than flagged pairs could need
-        const int64_t need = (x.class_pairs[c] + fp64_per_warp(c) - 1) / fp64_per_warp(c);
-        grid = std::min<int64_t>(grid, std::max<int64_t>(1, (need + kWarpsPerBlock - 1) / kWarpsPerBlock));
-        p.fp64_grid[c] = (int)grid;
     }
     p.scratch_bytes = (size_t)std::max<int64_t>(std::max(scratch, fp32_scratch), 256);
     return p;
@@ -853,16 +901,17 @@ pairhmm_status_t Engine::host_begin(const pairhmm_batch_t& b, float* scores, cud
     if (mark_end) PHMM_CUDA(cudaEventRecord(mark_end, s));
     // rescue counts and (into page-locked memory) scores come down now; scores
     // for pageable memory go through the uploader's slots in host_end
-    PHMM_CUDA(cudaMemcpyAsync(host_hdr_, counters_.as<unsigned long long>() + kMaxBuckets,
-                              sizeof(unsigned long long) * kFp64Classes, cudaMemcpyDeviceToHost, s));
+    PHMM_CUDA(cudaMemcpyAsync(host_hdr_, counters_.as<unsigned long long>() + kCtrScaled,
+                              sizeof(unsigned long long) * 2 * kFp64Classes, cudaMemcpyDeviceToHost, s));
     pend_direct_ = HostUploader::is_page_locked(scores);
     if (pend_direct_)
         PHMM_CUDA(cudaMemcpyAsync(scores, scores_.ptr, 4 * (size_t)x.num_pairs, cudaMemcpyDeviceToHost, s));
     pend_scores_ = scores;
     pend_pairs_ = x.num_pairs;
     stats_.h2d_bytes = 4 * rn + hn + 12 * x.num_reads + 12 * x.num_haps + index_bytes(x);
-    stats_.d2h_bytes = 4 * x.num_pairs + (int64_t)sizeof(unsigned long long) * kFp64Classes;
+    stats_.d2h_bytes = 4 * x.num_pairs + (int64_t)sizeof(unsigned long long) * 2 * kFp64Classes;
     stats_.launches = launches_;
+    stats_.fp32_launches = fp32_launches_;
     pending_ = true;
     return PAIRHMM_OK;
 }
@@ -875,8 +924,9 @@ pairhmm_status_t Engine::host_end() {
     if (!pend_direct_)
         PHMM_CUDA(uploader_.download(opts_.device, pend_scores_, scores_.ptr, 4 * (size_t)pend_pairs_, s));
     PHMM_CUDA(cudaStreamSynchronize(s));
-    unsigned long long rescued_by_class[kFp64Classes] = {};
-    static_assert(sizeof(rescued_by_class) <= 64, "rescue counts fit the landing spot");
+    // per class: the scaled tier's counts, then the extended tier's
+    unsigned long long rescued_by_class[2 * kFp64Classes] = {};
+    static_assert(sizeof(rescued_by_class) <= 256, "rescue counts fit the landing spot");
     std::memcpy(rescued_by_class, host_hdr_, sizeof(rescued_by_class));
     float ms = 0.f, a = 0.f, b2 = 0.f, c = 0.f;
     PHMM_CUDA(cudaEventElapsedTime(&ms, ev0_, ev1_));
@@ -888,7 +938,11 @@ pairhmm_status_t Engine::host_end() {
     stats_.fp32_ms = b2;
     stats_.fp64_ms = c;
     stats_.rescued = 0;
-    for (unsigned long long r : rescued_by_class) stats_.rescued += (int64_t)r;
+    stats_.rescued_ext = 0;
+    for (int c = 0; c < kFp64Classes; ++c) {
+        stats_.rescued += (int64_t)rescued_by_class[c];
+        stats_.rescued_ext += (int64_t)rescued_by_class[kFp64Classes + c];
+    }
     return PAIRHMM_OK;
 }
 
@@ -954,11 +1008,13 @@ pairhmm_status_t Engine::compute_host(const pairhmm_batch_t& b, float* scores) {
         sum.pairs += x.pairs;
         sum.cells += x.cells;
         sum.rescued += x.rescued;
+        sum.rescued_ext += x.rescued_ext;
         sum.multi_tile_pairs += x.multi_tile_pairs;
         sum.prep_ms += x.prep_ms;
         sum.fp32_ms += x.fp32_ms;
         sum.fp64_ms += x.fp64_ms;
         sum.launches += x.launches;
+        sum.fp32_launches += x.fp32_launches;
         sum.h2d_bytes += x.h2d_bytes;
         sum.d2h_bytes += x.d2h_bytes;
         return PAIRHMM_OK;
@@ -1037,6 +1093,7 @@ pairhmm_status_t Engine::compute_device(const pairhmm_batch_t& b, int32_t, int32
     stats_.cells = x.cells;
     stats_.multi_tile_pairs = x.multi_tile_pairs;
     stats_.rescued = -1;
+    stats_.rescued_ext = -1;
     if (x.num_pairs == 0) return PAIRHMM_OK;
     if (!scores) return fail(PAIRHMM_ERR_INVALID_ARGUMENT, "null scores");
     if ((st = ensure_buffers(x, false)) != PAIRHMM_OK) return st;

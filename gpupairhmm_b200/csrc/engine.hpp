@@ -104,7 +104,8 @@ private:
         int64_t rows = 0;                 // border rows per buffer
         std::vector<int> grid;            // by bucket
         std::vector<int> persistent;      // by bucket
-        int fp64_grid[kFp64Classes] = {};   // by FP64 length class
+        int fp64_grid[kFp64Classes] = {};   // by FP64 length class: scaled tier
+        int fp64_ext_grid[kFp64Classes] = {};  // extended tier
         std::vector<int64_t> scratch_off;   // by bucket: multi-tile kernels run side by side
         size_t scratch_bytes = 0;
     };
@@ -131,7 +132,7 @@ private:
     cudaStream_t side_[kSideStreams] = {};
     cudaEvent_t fork_ = nullptr, join_[kSideStreams] = {};
     cudaEvent_t ev0_ = nullptr, ev1_ = nullptr, ev_prep_ = nullptr, ev_fp32_ = nullptr;
-    int64_t launches_ = 0;
+    int64_t launches_ = 0, fp32_launches_ = 0;
     cudaGraphExec_t graph_exec_[3] = {nullptr, nullptr, nullptr};  // prep, FP32, FP64
     pairhmm_stats_t stats_{};
     std::string last_error_;
@@ -144,7 +145,7 @@ private:
     DevBuf read_record_, read_local_, rec_haps_, rec_hap_base_, rec_pair_base_, read_start_, hap_start_;
     DevBuf unit_read0_, unit_read1_, unit_bucket_;
     DevBuf read_pack_, hap_code_, hist_, cursor_, items_, rescue_, counters_, sched_, scores_, scratch_;
-    DevBuf lens_tmp_, rescue_off_;
+    DevBuf lens_tmp_, rescue_off_, rescue_ext_, rsort_;
     // host-to-device uploads (caller inputs, index) and the reused index
     HostUploader uploader_;
     BatchIndex idx_;
@@ -156,7 +157,7 @@ private:
     bool pending_ = false, pend_direct_ = false;
     float* pend_scores_ = nullptr;
     int64_t pend_pairs_ = 0;
-    // page-locked landing spot for the rescue counts
+    // page-locked landing spot for the rescue counts (both FP64 tiers)
     void* host_hdr_ = nullptr;
     // device memory pool of this engine's buffers (kept, not returned to the
     // system between batches)

@@ -32,6 +32,8 @@ struct Fp64LaunchArgs {
     DevView view;
     int cls;                         // length class (fp64_class)
     bool gcp;                        // gcp mode kernel
+    bool ext;                        // extended-range tier (per-lane exponents)
+    ExtList ext_list;                // scaled tier: where pairs beyond its range go
     const Task* items;               // that class's rescue list
     const unsigned long long* count; // number of items (device)
     unsigned long long* counter;     // task counter
@@ -59,19 +61,22 @@ struct ConfigInfo {
 const std::vector<ConfigInfo>& fp32_configs();
 const ConfigInfo* find_fp32_config(int G, int R, bool multi_tile, bool packed = false, bool gcp = false);
 
-// FP64 pass, one kernel per length class: (G, R) = (8, 8), (16, 8) single
-// tile and (32, 8) multi-tile.
-// gcp selects the gcp-mode kernels (eps/beta per read).
+// FP64 pass, one kernel per length class and tier (misc_kernels.cu): the
+// scaled tier (ext = false) recomputes every flagged pair, the extended tier
+// (ext = true) the pairs beyond the scaled tier's range.  gcp selects the
+// gcp-mode kernels (eps/beta per read).
 cudaError_t launch_fp64_rescue(const Fp64LaunchArgs& a);
-size_t fp64_smem_bytes(int cls);
-size_t fp64_scratch_bytes_per_row(int cls);  // per warp, per border row
-const void* fp64_kernel(int cls, bool gcp = false);
+size_t fp64_smem_bytes(int cls, bool ext);
+size_t fp64_scratch_bytes_per_row(int cls, bool ext);  // per warp, per border row
+const void* fp64_kernel(int cls, bool gcp, bool ext);
 int fp64_per_warp(int cls);
 
 // Preparation kernels.
 cudaError_t launch_pack(const PrepArgs& a, int grid, cudaStream_t s);
 // byte fills of n <= kFillRanges device ranges in one kernel launch
 cudaError_t launch_fill(uint8_t* const* ptr, const long long* bytes, const int* value, int n, cudaStream_t s);
+// FP64 class lists sorted by haplotype length (count, scan, scatter)
+cudaError_t launch_rescue_sort(const RescueSortArgs& a, int grid, cudaStream_t s);
 cudaError_t launch_binning(BinArgs a, int grid, cudaStream_t s, const int* per_task_dev,
                            const int* config_dev, Schedule* sched, int nranks);
 

@@ -45,35 +45,38 @@ const ConfigInfo* find_fp32_config(int G, int R, bool multi_tile, bool packed, b
 // workload -6%, of 250-bp reads -9%); 160 keeps 16 x 10 at 168 registers.
 // Multi-tile: 512-row tiles (32 x 16) halve the tiles of a long pair against
 // 32 x 8 (long-read workload's FP64 pass 38.3 -> 26.9 ms; one long-read
-// region's 11.5 -> 7.3 ms).
-using W64c0 = Fp64Wavefront<4, 16, false>;
-using W64c1 = Fp64Wavefront<8, 12, false>;
-using W64c2 = Fp64Wavefront<8, 16, false>;
-using W64c3 = Fp64Wavefront<16, 10, false>;
-using W64c4 = Fp64Wavefront<16, 12, false>;
-using W64c5 = Fp64Wavefront<16, 16, false>;
-using W64c6 = Fp64Wavefront<32, 16, true>;
-static_assert(W64c0::T == kFp64ClassMax[0] && W64c1::T == kFp64ClassMax[1] && W64c2::T == kFp64ClassMax[2] &&
-                  W64c3::T == kFp64ClassMax[3] && W64c4::T == kFp64ClassMax[4] && W64c5::T == kFp64ClassMax[5],
+// region's 11.5 -> 7.3 ms).  Both tiers use the same tiles: the scaled tier
+// (EXT = false) takes every flagged pair, the extended tier (EXT = true) the
+// few the scaled tier hands on.
+template <bool EXT> using W64c0 = Fp64Wavefront<4, 16, false, false, EXT>;
+template <bool EXT> using W64c1 = Fp64Wavefront<8, 12, false, false, EXT>;
+template <bool EXT> using W64c2 = Fp64Wavefront<8, 16, false, false, EXT>;
+template <bool EXT> using W64c3 = Fp64Wavefront<16, 10, false, false, EXT>;
+template <bool EXT> using W64c4 = Fp64Wavefront<16, 12, false, false, EXT>;
+template <bool EXT> using W64c5 = Fp64Wavefront<16, 16, false, false, EXT>;
+template <bool EXT> using W64c6 = Fp64Wavefront<32, 16, true, false, EXT>;
+static_assert(W64c0<true>::T == kFp64ClassMax[0] && W64c1<true>::T == kFp64ClassMax[1] &&
+                  W64c2<true>::T == kFp64ClassMax[2] && W64c3<true>::T == kFp64ClassMax[3] &&
+                  W64c4<true>::T == kFp64ClassMax[4] && W64c5<true>::T == kFp64ClassMax[5],
               "class bounds follow the tiles");
 
 template <class W>
 __global__ void __launch_bounds__(kBlockThreads, W::kMinCtas)
 fp64_rescue_kernel(DevView v, const Task* __restrict__ items, const unsigned long long* count,
-                   unsigned long long* counter, Border64* scratch, int64_t rows) {
+                   unsigned long long* counter, void* scratch, int64_t rows, ExtList ext) {
+    using Border = typename W::Border;
     extern __shared__ double2 smem64[];
     float* ph = reinterpret_cast<float*>(smem64);  // 128 floats = 32 double2
     const int warp = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
     double2* wtab = smem64 + 32 + warp * W::kTableDouble2;
-    Border64* ring = reinterpret_cast<Border64*>(smem64 + 32 + kWarpsPerBlock * W::kTableDouble2) +
-                     warp * W::kRing;
+    Border* ring = reinterpret_cast<Border*>(smem64 + 32 + kWarpsPerBlock * W::kTableDouble2) + warp * W::kRing;
     for (int i = threadIdx.x; i < 128; i += blockDim.x) ph[i] = v.ph2pr[i];
     __syncthreads();
     const unsigned long long n = *count;
     const unsigned long long ntasks = (n + W::NG - 1) / W::NG;
     const long long gwarp = (long long)blockIdx.x * kWarpsPerBlock + warp;
-    Border64* wscratch = scratch ? scratch + gwarp * 2 * rows : nullptr;
+    Border* wscratch = scratch ? static_cast<Border*>(scratch) + gwarp * rows : nullptr;
     while (true) {
         unsigned long long x = 0;
         if (lane == 0) x = atomicAdd(counter, 1ull);
@@ -81,54 +84,66 @@ fp64_rescue_kernel(DevView v, const Task* __restrict__ items, const unsigned lon
         if (x >= ntasks) break;
         const unsigned long long first = x * W::NG;
         const int ntask = (int)((n - first) < (unsigned long long)W::NG ? (n - first) : W::NG);
-        W::run(v, items + first, ntask, ph, wtab, ring, wscratch, rows);
+        W::run(v, items + first, ntask, ph, wtab, ring, wscratch, rows, ext);
     }
 }
 
 template <class W>
 size_t fp64_smem_for() {
     return (32 + (size_t)kWarpsPerBlock * W::kTableDouble2) * sizeof(double2) +
-           (size_t)kWarpsPerBlock * W::kRing * sizeof(Border64);
+           (size_t)kWarpsPerBlock * W::kRing * sizeof(typename W::Border);
 }
 
 // gcp-mode twins of the class kernels (same tiles, eps/beta per read)
 template <class W>
 struct WithGcp;
-template <int G, int R, bool MT>
-struct WithGcp<Fp64Wavefront<G, R, MT, false>> {
-    using type = Fp64Wavefront<G, R, MT, true>;
+template <int G, int R, bool MT, bool EXT>
+struct WithGcp<Fp64Wavefront<G, R, MT, false, EXT>> {
+    using type = Fp64Wavefront<G, R, MT, true, EXT>;
 };
 
-#define PHMM_FP64_DISPATCH(cls, EXPR)      \
-    switch (cls) {                          \
-        case 0: { using W = W64c0; EXPR; }  \
-        case 1: { using W = W64c1; EXPR; }  \
-        case 2: { using W = W64c2; EXPR; }  \
-        case 3: { using W = W64c3; EXPR; }  \
-        case 4: { using W = W64c4; EXPR; }  \
-        case 5: { using W = W64c5; EXPR; }  \
-        default: { using W = W64c6; EXPR; } \
+#define PHMM_FP64_DISPATCH_T(cls, X, EXPR)    \
+    switch (cls) {                             \
+        case 0: { using W = W64c0<X>; EXPR; }  \
+        case 1: { using W = W64c1<X>; EXPR; }  \
+        case 2: { using W = W64c2<X>; EXPR; }  \
+        case 3: { using W = W64c3<X>; EXPR; }  \
+        case 4: { using W = W64c4<X>; EXPR; }  \
+        case 5: { using W = W64c5<X>; EXPR; }  \
+        default: { using W = W64c6<X>; EXPR; } \
     }
+#define PHMM_FP64_DISPATCH(cls, ext, EXPR)                               \
+    do {                                                                 \
+        if (ext) { PHMM_FP64_DISPATCH_T(cls, true, EXPR) }               \
+        else { PHMM_FP64_DISPATCH_T(cls, false, EXPR) }                  \
+    } while (0)
 
 // the gcp twin has the same tables and ring, so the same shared memory
-size_t fp64_smem_bytes(int cls) { PHMM_FP64_DISPATCH(cls, return fp64_smem_for<W>()); }
-size_t fp64_scratch_bytes_per_row(int cls) { return cls == kFp64Classes - 1 ? 2 * sizeof(Border64) : 0; }
-const void* fp64_kernel(int cls, bool gcp) {
-    PHMM_FP64_DISPATCH(cls, return gcp ? reinterpret_cast<const void*>(&fp64_rescue_kernel<typename WithGcp<W>::type>)
-                                       : reinterpret_cast<const void*>(&fp64_rescue_kernel<W>));
+size_t fp64_smem_bytes(int cls, bool ext) { PHMM_FP64_DISPATCH(cls, ext, return fp64_smem_for<W>()); }
+// one border buffer per warp, shared by all tile boundaries of its pair
+size_t fp64_scratch_bytes_per_row(int cls, bool ext) {
+    if (cls != kFp64Classes - 1) return 0;
+    return ext ? sizeof(Border64) : sizeof(Border64S);
 }
-int fp64_per_warp(int cls) { PHMM_FP64_DISPATCH(cls, return W::NG); }
+const void* fp64_kernel(int cls, bool gcp, bool ext) {
+    PHMM_FP64_DISPATCH(cls, ext,
+                       return gcp ? reinterpret_cast<const void*>(&fp64_rescue_kernel<typename WithGcp<W>::type>)
+                                  : reinterpret_cast<const void*>(&fp64_rescue_kernel<W>));
+}
+int fp64_per_warp(int cls) { PHMM_FP64_DISPATCH(cls, true, return W::NG); }
 
 cudaError_t launch_fp64_rescue(const Fp64LaunchArgs& a) {
-    Border64* scr = a.cls == kFp64Classes - 1 ? static_cast<Border64*>(a.scratch) : nullptr;
+    void* scr = a.cls == kFp64Classes - 1 ? a.scratch : nullptr;
+    const size_t smem = fp64_smem_bytes(a.cls, a.ext);
     if (a.gcp) {
-        PHMM_FP64_DISPATCH(a.cls, (fp64_rescue_kernel<typename WithGcp<W>::type>
-                                   <<<a.grid, kBlockThreads, fp64_smem_bytes(a.cls), a.stream>>>(
-                                       a.view, a.items, a.count, a.counter, scr, a.rows));
+        PHMM_FP64_DISPATCH(a.cls, a.ext,
+                           (fp64_rescue_kernel<typename WithGcp<W>::type><<<a.grid, kBlockThreads, smem, a.stream>>>(
+                                a.view, a.items, a.count, a.counter, scr, a.rows, a.ext_list));
                            return cudaGetLastError());
     }
-    PHMM_FP64_DISPATCH(a.cls, (fp64_rescue_kernel<W><<<a.grid, kBlockThreads, fp64_smem_bytes(a.cls), a.stream>>>(
-                                   a.view, a.items, a.count, a.counter, scr, a.rows));
+    PHMM_FP64_DISPATCH(a.cls, a.ext,
+                       (fp64_rescue_kernel<W><<<a.grid, kBlockThreads, smem, a.stream>>>(
+                            a.view, a.items, a.count, a.counter, scr, a.rows, a.ext_list));
                        return cudaGetLastError());
 }
 
@@ -157,6 +172,13 @@ cudaError_t launch_fill(uint8_t* const* ptr, const long long* bytes, const int* 
     if (most == 0) return cudaSuccess;
     const long long blocks = (most + 255) / 256;
     fill_kernel<<<(int)(blocks < 1024 ? blocks : 1024), 256, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_rescue_sort(const RescueSortArgs& a, int grid, cudaStream_t s) {
+    rescue_count_kernel<<<grid, 256, 0, s>>>(a);
+    rescue_scan_kernel<<<1, 32 * kFp64Classes, 0, s>>>(a);
+    rescue_scatter_kernel<<<grid, 256, 0, s>>>(a);
     return cudaGetLastError();
 }
 

@@ -28,7 +28,6 @@
 
 #include <atomic>
 #include <cfloat>
-#include <cmath>
 #include <cstdint>
 #include <mutex>
 
@@ -50,8 +49,11 @@ constexpr int kMaxDevices = 64;
 static __device__ __align__(256) float4 g_scratch[kScratchBytes / sizeof(float4)];
 
 // probability table p(q) = float(10^(-q/10)) (gpuworker.cuh:473-486), in
-// constant memory of this module; uploaded at set-up
-static __constant__ float c_ph2pr[128];
+// constant memory of this module, initialised in the module image itself: no
+// upload, so a context that is torn down and created again has it too
+static __constant__ float c_ph2pr[128] = {
+#include "ph2pr_table.inc"
+};
 
 __device__ __forceinline__ uint32_t encode(uint8_t c) {
     return c == 'A' ? 0u : c == 'C' ? 1u : c == 'G' ? 2u : c == 'T' ? 3u : 4u;
@@ -189,33 +191,31 @@ forward_pairs_kernel(const uint8_t* __restrict__ read_bases, const uint8_t* __re
     }
 }
 
-// per-device set-up: symbol address of the scratch, table upload, grid size
+// per-device set-up: the scratch array's device address and the grid size
 struct DeviceState {
     std::atomic<int> ready{0};
-    float4* scratch = nullptr;
+    std::atomic<float4*> scratch{nullptr};
     int max_warps = 0;
 };
 DeviceState g_state[kMaxDevices];
 std::mutex g_setup_mutex;
 
 // Runs once per device, with that device current (the caller makes it so):
-// looks up the scratch array's device address, uploads the probability table
-// and sizes the grid.  Nothing here allocates.
+// looks up the scratch array's device address (in host code the array's name
+// is only a host-side stand-in) and sizes the grid from the SM count and the
+// kernel's occupancy.  Nothing here allocates.
 pairhmm_status_t setup(int device, DeviceState& st) {
     std::lock_guard<std::mutex> lk(g_setup_mutex);
     if (st.ready.load()) return PAIRHMM_OK;
     float4* addr = nullptr;
     if (cudaGetSymbolAddress(reinterpret_cast<void**>(&addr), g_scratch) != cudaSuccess || addr == nullptr)
         return PAIRHMM_ERR_CUDA;
-    float table[128];
-    for (int i = 0; i < 128; ++i) table[i] = (float)std::pow(10.0, (-i) / 10.0);
-    if (cudaMemcpyToSymbol(c_ph2pr, table, sizeof(table)) != cudaSuccess) return PAIRHMM_ERR_CUDA;
+    st.scratch.store(addr);
     int sms = 0, per_sm = 0;
     if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) return PAIRHMM_ERR_CUDA;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, forward_pairs_kernel, kThreads, 0) != cudaSuccess ||
         per_sm < 1)
         per_sm = 1;
-    st.scratch = addr;
     st.max_warps = sms * per_sm * (kThreads / 32);
     st.ready.store(1);
     return PAIRHMM_OK;
@@ -240,6 +240,14 @@ extern "C" pairhmm_status_t pairhmm_forward_pairs_noalloc(
     if (prev != device && cudaSetDevice(device) != cudaSuccess) return PAIRHMM_ERR_CUDA;
     DeviceState& st = g_state[device];
     pairhmm_status_t status = st.ready.load() ? PAIRHMM_OK : setup(device, st);
+    // the set-up's address is checked against a fresh lookup on every call (a
+    // symbol lookup, no allocation): after the context was torn down and created
+    // again the module, and the array with it, may sit elsewhere
+    float4* scratch = nullptr;
+    if (status == PAIRHMM_OK &&
+        (cudaGetSymbolAddress(reinterpret_cast<void**>(&scratch), g_scratch) != cudaSuccess || !scratch))
+        status = PAIRHMM_ERR_CUDA;
+    if (status == PAIRHMM_OK && scratch != st.scratch.load()) st.scratch.store(scratch);
     if (status == PAIRHMM_OK) {
         // border rows per buffer for this call, and how many warps the scratch holds
         const int64_t rows = ((int64_t)max_hap_length + 2 * kG + 8 + 63) / 64 * 64;
@@ -249,10 +257,18 @@ extern "C" pairhmm_status_t pairhmm_forward_pairs_noalloc(
         if (warps > num_pairs) warps = num_pairs;
         const int64_t warps_per_block = kThreads / 32;
         const int grid = (int)((warps + warps_per_block - 1) / warps_per_block);
-        forward_pairs_kernel<<<grid, kThreads, 0, static_cast<cudaStream_t>(stream)>>>(
-            read_bases, base_quals, ins_quals, del_quals, hap_bases, pairs, num_pairs, scores, st.scratch, rows,
-            warps, max_hap_length);
-        status = cudaGetLastError() == cudaSuccess ? PAIRHMM_OK : PAIRHMM_ERR_CUDA;
+        // cudaLaunchKernel returns this launch's own status, so an error the caller
+        // left pending is neither reported as ours nor cleared
+        int max_h = max_hap_length;
+        int64_t np = num_pairs;
+        void* args[] = {(void*)&read_bases, (void*)&base_quals, (void*)&ins_quals, (void*)&del_quals,
+                        (void*)&hap_bases, (void*)&pairs, &np, &scores, &scratch, (void*)&rows, &warps, &max_h};
+        const cudaError_t le = cudaLaunchKernel(reinterpret_cast<const void*>(&forward_pairs_kernel), dim3(grid),
+                                                dim3(kThreads), args, 0, static_cast<cudaStream_t>(stream));
+        if (le != cudaSuccess) {
+            cudaGetLastError();  // the failed launch's own error, recorded by the runtime as well
+            status = PAIRHMM_ERR_CUDA;
+        }
     }
     if (prev != device) cudaSetDevice(prev);
     return status;

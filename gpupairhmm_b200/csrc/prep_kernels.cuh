@@ -216,7 +216,7 @@ __global__ void bin_scatter_kernel(BinArgs a) {
 // Byte fills of up to kFillRanges device ranges in one launch.  Used instead of
 // cudaMemsetAsync inside the captured stages: a memset node may be run by a
 // copy engine, where it queues behind other streams' pending copies.
-constexpr int kFillRanges = 3;
+constexpr int kFillRanges = 4;
 struct FillArgs {
     uint8_t* ptr[kFillRanges];
     long long bytes[kFillRanges];
@@ -286,6 +286,80 @@ __global__ void schedule_kernel(const unsigned long long* bin_start, const unsig
     }
     s->task_begin[nranks] = tasks;
     s->total_tasks = tasks;
+}
+#endif  // PHMM_PREP_KERNELS_IMPL
+
+// ---------------------------------------------------------------- FP64 list order
+// The FP32 pass appends flagged pairs to the FP64 class lists in completion
+// order, so the pairs of one FP64 warp task (NG of them) would have unrelated
+// haplotype lengths and the warp would run as long as the longest.  A counting
+// sort by haplotype length (descending, 16-position classes; longer than
+// 8,175 in the last class) makes consecutive pairs alike, as the FP32 work
+// list is: count, per-class scan, scatter into a second list with the same
+// class offsets.
+constexpr int kRescueHBins = 512;
+struct RescueSortArgs {
+    const Task* in;                   // class lists in append order
+    Task* out;                        // the same lists, sorted
+    const long long* off;             // [kFp64Classes] list starts
+    const unsigned long long* count;  // [kFp64Classes] list lengths
+    const int32_t* hap_len;
+    unsigned int* hist;               // [kFp64Classes * kRescueHBins], zeroed before the batch
+    unsigned long long* cursor;       // [kFp64Classes * kRescueHBins]
+};
+
+__device__ __forceinline__ int rescue_hbin(int H) {
+    const int b = H >> 4;
+    return kRescueHBins - 1 - (b < kRescueHBins - 1 ? b : kRescueHBins - 1);
+}
+
+#ifdef PHMM_PREP_KERNELS_IMPL
+__global__ void rescue_count_kernel(RescueSortArgs a) {
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (int c = 0; c < kFp64Classes; ++c) {
+        const long long n = (long long)a.count[c];
+        const Task* in = a.in + a.off[c];
+        for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+            const int bin = c * kRescueHBins + rescue_hbin(a.hap_len[in[i].hap]);
+            aggregated_add(&a.hist[bin], (unsigned)bin);
+        }
+    }
+}
+
+// one warp per class: exclusive scan of its bins (16 per lane) from the list start
+__global__ void __launch_bounds__(32 * kFp64Classes) rescue_scan_kernel(RescueSortArgs a) {
+    constexpr int kPer = kRescueHBins / 32;
+    const int c = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const unsigned int* h = a.hist + c * kRescueHBins + lane * kPer;
+    unsigned long long sum = 0;
+#pragma unroll
+    for (int i = 0; i < kPer; ++i) sum += h[i];
+    unsigned long long incl = sum;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const unsigned long long y = __shfl_up_sync(kFullMask, incl, d);
+        if (lane >= d) incl += y;
+    }
+    unsigned long long run = (unsigned long long)a.off[c] + incl - sum;
+    unsigned long long* cur = a.cursor + c * kRescueHBins + lane * kPer;
+#pragma unroll
+    for (int i = 0; i < kPer; ++i) {
+        cur[i] = run;
+        run += h[i];
+    }
+}
+
+__global__ void rescue_scatter_kernel(RescueSortArgs a) {
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (int c = 0; c < kFp64Classes; ++c) {
+        const long long n = (long long)a.count[c];
+        const Task* in = a.in + a.off[c];
+        for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+            const Task t = in[i];
+            const int bin = c * kRescueHBins + rescue_hbin(a.hap_len[t.hap]);
+            a.out[aggregated_add(&a.cursor[bin], (unsigned)bin)] = t;
+        }
+    }
 }
 #endif  // PHMM_PREP_KERNELS_IMPL
 

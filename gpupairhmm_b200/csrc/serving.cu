@@ -27,6 +27,27 @@ ServingQueue::~ServingQueue() {
     for (auto& t : threads_) t.join();
 }
 
+pairhmm_status_t ServingQueue::set_error(pairhmm_status_t s, const char* msg) {
+    error_ = msg;
+    return s;
+}
+
+std::string ServingQueue::last_error() {
+    std::lock_guard<std::mutex> lk(mu_);
+    return error_;
+}
+
+void ServingQueue::stats(pairhmm_serving_stats_t* out) {
+    std::lock_guard<std::mutex> lk(mu_);
+    out->regions = regions_done_;
+    out->batches = batches_;
+    out->max_batch_regions = max_batch_regions_;
+    out->max_batch_bytes = max_batch_bytes_;
+    out->budget_per_slot = budget_per_slot_;
+    out->slots = kSlots;
+    out->max_in_flight = max_in_flight_;
+}
+
 int64_t ServingQueue::estimate_device_bytes(const Region& r) {
     // inputs (4 byte arrays + haplotypes), packed copies, work items, rescue
     // list and scores, plus the per-read/per-haplotype index arrays
@@ -43,21 +64,20 @@ pairhmm_status_t ServingQueue::submit(const pairhmm_batch_t& b, uint64_t* ticket
     std::string err;
     pairhmm_status_t st = Engine::build_index(b, parent_.tile_table(), x, err);
     if (st != PAIRHMM_OK) {
-        error_ = err;
-        return st;
-    }
-    if (x.num_reads > 0 && (!b.read_bases || !b.base_quals || !b.ins_quals || !b.del_quals || !b.read_offsets)) {
-        error_ = "null read arrays";
-        return PAIRHMM_ERR_INVALID_ARGUMENT;
-    }
-    if (x.num_haps > 0 && (!b.hap_bases || !b.hap_offsets)) {
-        error_ = "null haplotype arrays";
-        return PAIRHMM_ERR_INVALID_ARGUMENT;
+        std::lock_guard<std::mutex> lk(mu_);
+        return set_error(st, err.c_str());
     }
     const bool gcp = parent_.gcp();
-    if (gcp && x.num_reads > 0 && !b.gcp_quals) {
-        error_ = "gcp mode needs the gcp quality array";
-        return PAIRHMM_ERR_INVALID_ARGUMENT;
+    const char* bad = nullptr;
+    if (x.num_reads > 0 && (!b.read_bases || !b.base_quals || !b.ins_quals || !b.del_quals || !b.read_offsets))
+        bad = "null read arrays";
+    else if (x.num_haps > 0 && (!b.hap_bases || !b.hap_offsets))
+        bad = "null haplotype arrays";
+    else if (gcp && x.num_reads > 0 && !b.gcp_quals)
+        bad = "gcp mode needs the gcp quality array";
+    if (bad) {
+        std::lock_guard<std::mutex> lk(mu_);
+        return set_error(PAIRHMM_ERR_INVALID_ARGUMENT, bad);
     }
     auto r = std::make_shared<Region>();
     r->rpr.assign(b.reads_per_record, b.reads_per_record + b.num_records);
@@ -91,8 +111,8 @@ pairhmm_status_t ServingQueue::submit(const pairhmm_batch_t& b, uint64_t* ticket
     r->heavy = x.max_read_len > single_tile_max_;
     r->device_bytes = estimate_device_bytes(*r);
     if (r->device_bytes > budget_per_slot_) {
-        error_ = "region needs more device memory than one batch slot's budget";
-        return PAIRHMM_ERR_BUDGET;
+        std::lock_guard<std::mutex> lk(mu_);
+        return set_error(PAIRHMM_ERR_BUDGET, "region needs more device memory than one batch slot's budget");
     }
     r->t_submit = std::chrono::steady_clock::now();
     {
@@ -112,7 +132,7 @@ pairhmm_status_t ServingQueue::submit(const pairhmm_batch_t& b, uint64_t* ticket
                 if (is != PAIRHMM_OK) {
                     error_ = e->last_error();
                     engines_.clear();
-                    return is;
+                    return is;  // mu_ is held: error_ is written under it
                 }
                 engines_.push_back(std::move(e));
             }
@@ -155,6 +175,10 @@ void ServingQueue::worker(int slot) {
                 queue.pop_front();
             }
             more = !queue.empty();
+            ++batches_;
+            max_batch_regions_ = std::max<int64_t>(max_batch_regions_, (int64_t)take.size());
+            max_batch_bytes_ = std::max(max_batch_bytes_, bytes);
+            max_in_flight_ = std::max(max_in_flight_, ++in_flight_);
         }
         if (more) cv_work_.notify_all();
         // merge the regions into one batch
@@ -198,6 +222,8 @@ void ServingQueue::worker(int slot) {
         const auto now = std::chrono::steady_clock::now();
         {
             std::lock_guard<std::mutex> lk(mu_);
+            --in_flight_;
+            regions_done_ += (int64_t)take.size();
             int64_t off = 0;
             for (const auto& r : take) {
                 r->status = st;
@@ -215,10 +241,7 @@ void ServingQueue::worker(int slot) {
 pairhmm_status_t ServingQueue::poll(uint64_t ticket, int32_t* done) {
     std::lock_guard<std::mutex> lk(mu_);
     auto it = tickets_.find(ticket);
-    if (it == tickets_.end()) {
-        error_ = "unknown ticket";
-        return PAIRHMM_ERR_NOT_FOUND;
-    }
+    if (it == tickets_.end()) return set_error(PAIRHMM_ERR_NOT_FOUND, "unknown ticket");
     *done = it->second->done ? 1 : 0;
     return PAIRHMM_OK;
 }
@@ -226,14 +249,8 @@ pairhmm_status_t ServingQueue::poll(uint64_t ticket, int32_t* done) {
 pairhmm_status_t ServingQueue::latency(uint64_t ticket, double* ms) {
     std::lock_guard<std::mutex> lk(mu_);
     auto it = tickets_.find(ticket);
-    if (it == tickets_.end()) {
-        error_ = "unknown ticket";
-        return PAIRHMM_ERR_NOT_FOUND;
-    }
-    if (!it->second->done) {
-        error_ = "region not finished";
-        return PAIRHMM_ERR_BUSY;
-    }
+    if (it == tickets_.end()) return set_error(PAIRHMM_ERR_NOT_FOUND, "unknown ticket");
+    if (!it->second->done) return set_error(PAIRHMM_ERR_BUSY, "region not finished");
     *ms = std::chrono::duration<double, std::milli>(it->second->t_done - it->second->t_submit).count();
     return PAIRHMM_OK;
 }
@@ -241,27 +258,24 @@ pairhmm_status_t ServingQueue::latency(uint64_t ticket, double* ms) {
 pairhmm_status_t ServingQueue::drain(uint64_t ticket, float* scores, int64_t num_scores, int32_t timeout_ms) {
     std::unique_lock<std::mutex> lk(mu_);
     auto it = tickets_.find(ticket);
-    if (it == tickets_.end()) {
-        error_ = "unknown ticket";
-        return PAIRHMM_ERR_NOT_FOUND;
-    }
+    if (it == tickets_.end()) return set_error(PAIRHMM_ERR_NOT_FOUND, "unknown ticket");
     std::shared_ptr<Region> r = it->second;
     if (timeout_ms < 0) cv_done_.wait(lk, [&] { return r->done; });
-    else if (!cv_done_.wait_for(lk, std::chrono::milliseconds(timeout_ms), [&] { return r->done; })) {
-        error_ = "timed out waiting for the region";
-        return PAIRHMM_ERR_TIMEOUT;
-    }
+    else if (!cv_done_.wait_for(lk, std::chrono::milliseconds(timeout_ms), [&] { return r->done; }))
+        return set_error(PAIRHMM_ERR_TIMEOUT, "timed out waiting for the region");
+    // the wait released mu_: another thread may have drained this ticket meanwhile,
+    // so the map entry is looked up again rather than reused
+    if (tickets_.find(ticket) == tickets_.end())
+        return set_error(PAIRHMM_ERR_NOT_FOUND, "ticket drained by another call");
     if (r->status != PAIRHMM_OK) {
         error_ = r->error;
-        tickets_.erase(it);
+        tickets_.erase(ticket);
         return r->status;
     }
-    if (num_scores < r->pairs) {
-        error_ = "score buffer smaller than the region's pair count";
-        return PAIRHMM_ERR_INVALID_ARGUMENT;
-    }
+    if (num_scores < r->pairs)
+        return set_error(PAIRHMM_ERR_INVALID_ARGUMENT, "score buffer smaller than the region's pair count");
     std::copy(r->scores.begin(), r->scores.end(), scores);
-    tickets_.erase(it);
+    tickets_.erase(ticket);
     return PAIRHMM_OK;
 }
 

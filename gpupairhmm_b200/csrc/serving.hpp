@@ -38,7 +38,9 @@ public:
     pairhmm_status_t poll(uint64_t ticket, int32_t* done);
     pairhmm_status_t drain(uint64_t ticket, float* scores, int64_t num_scores, int32_t timeout_ms);
     pairhmm_status_t latency(uint64_t ticket, double* ms);
-    const std::string& last_error() const { return error_; }
+    void stats(pairhmm_serving_stats_t* out);
+    // the last error of any call (a copy: calls may come from several threads)
+    std::string last_error();
 
     static constexpr int kLightSlots = 2;          // regions of single-tile reads
     static constexpr int kSlots = kLightSlots + 1;  // + one slot for multi-tile regions
@@ -61,6 +63,7 @@ private:
 
     void worker(int slot);
     static int64_t estimate_device_bytes(const Region& r);
+    pairhmm_status_t set_error(pairhmm_status_t s, const char* msg);  // caller holds mu_
 
     Engine& parent_;
     int64_t budget_per_slot_ = 0;
@@ -74,6 +77,9 @@ private:
     uint64_t next_ticket_ = 1;
     bool stop_ = false;
     std::string error_;
+    // admission record (under mu_)
+    int64_t batches_ = 0, regions_done_ = 0, max_batch_regions_ = 0, max_batch_bytes_ = 0;
+    int32_t in_flight_ = 0, max_in_flight_ = 0;
 };
 
 }  // namespace phmm

@@ -1,10 +1,21 @@
 // FP64 pass: the same wavefront in double precision for the pairs the FP32
 // pass flagged (scaled FP32 sum below the underflow threshold, or an alpha
-// too close to zero for the FP32 kernel's division).
+// too close to zero for the FP32 kernel's division).  Two tiers:
 //
-// Range: an unrelated 250 bp read against a 600 bp haplotype lies ~244
-// decades below 1 and long reads reach thousands of decades, beyond a
-// pre-scaled double.  Every lane therefore stores its values as
+// Scaled tier (EXT = false): plain doubles under one fixed power-of-two scale.
+// The D boundary enters at 2^kScaledExp times the reference's FLT_MAX/16 scale
+// (values start near 2^960, leaving 2^63 of headroom for the rescaled
+// variables, which exceed the true values by at most 1/q and 1/s < 2^45).  A
+// cell's share of the result is at most its value, and each of the five
+// roundings of a cell moves a true value by at most 2^-1075 in the subnormal
+// range, so a sum S >= L*H*2^-1030 is exact to 5*2^-45 relative; that covers
+// pairs down to about 10^-599 * L*H.  Pairs below it (or non-finite) go on to
+// the extended tier's list.  No exponent bookkeeping: a step is the R cells,
+// the hand-off shuffles and the table loads.
+//
+// Extended tier (EXT = true): an unrelated read far longer than its haplotype
+// lies thousands of decades below 1, beyond a pre-scaled double.  Every lane
+// therefore stores its values as
 // true * 2^e  with its own integer exponent e.  A lane centres its exponent
 // on the first non-zero values it receives (its neighbour may not have
 // renormalised yet), every 16 steps it renormalises its registers by an exact
@@ -29,26 +40,47 @@
 // alpha, so pairs with alpha near or at zero are exact here.  The read-end
 // carry is that of the FP32 kernel (eps = 1 and scale beta from the read end).
 //
-// The recurrence is the plain one (alpha kept, not divided out), so pairs
-// with alpha ~ 0 are exact here.  Work split as in the FP32 kernel: groups of
-// G lanes, R doubles per lane, T = G*R read positions per tile; reads longer
-// than T (MT, G = 32 only) run tile after tile with the last lane's
-// (M, Dt, It, exponents) per haplotype row going through a global border
-// buffer, staged through a 32-entry shared ring for lane 0 of the next tile.
+// Work split as in the FP32 kernel: groups of G lanes, R doubles per lane,
+// T = G*R read positions per tile; reads longer than T (MT, G = 32 only) run
+// tile after tile with the last lane's (M, Dt, It, exponents) per haplotype
+// row going through a global border buffer, staged through a 32-entry shared
+// ring for lane 0 of the next tile.  One buffer serves every tile boundary of
+// a pair: tile i+1 reads a row (ring prefetch, up to 64 rows ahead) before its
+// own last lane overwrites it 31 steps later, in the same warp.
 #pragma once
 
 #include <climits>
+#include <type_traits>
 
 #include "device_common.cuh"
 
 namespace phmm {
 
+// Border row between read tiles: M of row s, X^ and I^ of row s + 1.  The
+// extended tier carries the exponents too; the scaled tier needs none.
 struct Border64 {
     double m, x, i;
     int e;   // exponent of m (row s)
     int ei;  // exponent of x and i (row s + 1)
 };
 static_assert(sizeof(Border64) == 32, "Border64 is 32 bytes");
+struct Border64S {
+    double m, x, i;
+};
+static_assert(sizeof(Border64S) == 24, "Border64S is 24 bytes");
+
+template <bool EXT>
+__device__ __forceinline__ void border_set_m(Border64& b, double m, int e) { b.m = m; b.e = e; }
+template <bool EXT>
+__device__ __forceinline__ void border_set_m(Border64S& b, double m, int) { b.m = m; }
+template <bool EXT>
+__device__ __forceinline__ void border_set_xi(Border64& b, double x, double i, int e) { b.x = x; b.i = i; b.ei = e; }
+template <bool EXT>
+__device__ __forceinline__ void border_set_xi(Border64S& b, double x, double i, int) { b.x = x; b.i = i; }
+__device__ __forceinline__ int border_e(const Border64& b) { return b.e; }
+__device__ __forceinline__ int border_e(const Border64S&) { return 0; }
+__device__ __forceinline__ int border_ei(const Border64& b) { return b.ei; }
+__device__ __forceinline__ int border_ei(const Border64S&) { return 0; }
 
 // 2^k as a double for k clamped to the normal range (exact power of two)
 __device__ __forceinline__ double pow2i(int k) {
@@ -56,7 +88,15 @@ __device__ __forceinline__ double pow2i(int k) {
     return __longlong_as_double((long long)(k + 1023) << 52);
 }
 
-template <int G, int R, bool MT, bool GCP = false>
+// Scaled tier: the D boundary's power-of-two factor over the reference's scale,
+// and the smallest sum it keeps (relative error of the subnormal roundings
+// below 5*2^-45 above it).
+constexpr int kScaledExp = 836;
+__host__ __device__ __forceinline__ double scaled_tier_threshold(int L, int H) {
+    return (double)L * (double)H * 0x1p-1030;
+}
+
+template <int G, int R, bool MT, bool GCP = false, bool EXT = true>
 struct Fp64Wavefront {
     static_assert(R % 2 == 0, "R must be even");
     static_assert(!MT || G == 32, "multi-tile FP64 runs one pair per warp");
@@ -65,6 +105,7 @@ struct Fp64Wavefront {
     static constexpr int Q = R / 2;                   // double2 per thread per table row
     static constexpr int kTableDouble2 = 5 * Q * 32;  // per warp
     static constexpr int kRing = 32;
+    using Border = typename std::conditional<EXT, Border64, Border64S>::type;
     // largest scale difference a hand-off converts: stored values stay within
     // about 2^(64 + 13*16) of 1 between renormalisations, so 2^640 more keeps
     // every converted value below 2^1023
@@ -76,9 +117,10 @@ struct Fp64Wavefront {
     static constexpr int kMinCtas = R == 10 ? 6 : (R == 8 && !MT) ? 8 : 1;
 
     // tasks: the warp's ntask (<= NG) items.  wtab: this warp's lambda table;
-    // ring: kRing shared entries (MT); scratch: this warp's 2 x rows Border64.
+    // ring: kRing shared entries (MT); scratch: this warp's rows border entries.
+    // ext: the extended tier's lists (scaled tier only).
     __device__ static void run(const DevView& v, const Task* tasks, int ntask, const float* ph, double2* wtab,
-                               Border64* ring, Border64* scratch, int64_t rows) {
+                               Border* ring, Border* scratch, int64_t rows, const ExtList& ext) {
         const int lane = threadIdx.x & 31;
         const int grp = lane / G;
         const int t = lane - grp * G;
@@ -97,11 +139,12 @@ struct Fp64Wavefront {
         const float eps_f = GCP ? ph[v.read_gcp[task.read]] : kEps;
         const double beta = GCP ? (double)(float)(1.0 - (double)eps_f) : (double)kBeta;
         const double epsd = (double)eps_f;
-        const double Dbound = beta * (double)(kScale / (float)Hc);
+        const double Dbound = beta * (double)(kScale / (float)Hc) * (EXT ? 1.0 : 0x1p836);
+        static_assert(kScaledExp == 836, "scale literal");
 
         double acc = 0.0;
-        int e = 0;
-        int eacc = 0;  // exponent of acc: the lane's e up to the pair's last step, then frozen
+        int e = EXT ? 0 : kScaledExp;
+        int eacc = e;  // exponent of acc: the lane's e up to the pair's last step, then frozen
         int rlane = -1;
 
         for (int tile = 0; tile < ntiles; ++tile) {
@@ -143,7 +186,7 @@ struct Fp64Wavefront {
 #pragma unroll
                 for (int h = 0; h < 5; ++h) wtab[(h * Q + q) * 32 + lane] = make_double2(lam[h][0], lam[h][1]);
             }
-            e = 0;
+            if constexpr (EXT) e = 0;
             int t_res = 0, r_res = 0;
             if (last) {
                 const int rel = Lc - 1 - tile * T;
@@ -166,10 +209,10 @@ struct Fp64Wavefront {
             int eMl = 0, eMul = 0, eIul = 0;
             if (t == 0 && tile == 0) Xul = Dbound;
             bool empty = !(t == 0 && tile == 0);
-            const Border64* ein = scratch + ((tile - 1) & 1) * rows;
-            Border64* eout = scratch + (tile & 1) * rows;
+            const Border* ein = scratch;
+            Border* eout = scratch;
             const bool writer = MT && valid && !last && t == G - 1;
-            Border64 nb{0.0, 0.0, 0.0, 0, 0};
+            Border nb{};
             if (MT && tile > 0 && t < rows) nb = ein[t];
             int h = 4;
 
@@ -193,14 +236,14 @@ struct Fp64Wavefront {
                     if (t == 0) hn = (int)((wcur >> (8 * s)) & 0xffu);
                     h = hn;
                     // lanes fill during the first pass of the wavefront (k < G + 8)
-                    if (k0 < G + 8 && empty && (Mul != 0.0 || Xul != 0.0 || Iul != 0.0)) {
+                    if (EXT && k0 < G + 8 && empty && (Mul != 0.0 || Xul != 0.0 || Iul != 0.0)) {
                         // centre this lane's scale on the first values it receives
                         const double xi = fmax(fabs(Xul), fabs(Iul));
                         e = Mul != 0.0 ? eMul - ilogb(fabs(Mul)) : eIul - ilogb(xi);
                         empty = false;
                     }
                     const double2* trow = wtab + h * (Q * 32) + lane;
-                    if (e - (eMul < eIul ? eMul : eIul) > kMaxShift) {  // rare: one compare per step
+                    if (EXT && e - (eMul < eIul ? eMul : eIul) > kMaxShift) {  // rare: one compare per step
                         // a neighbour's values far above this lane's scale (a lane centred on
                         // the tiny first values of a long insertion path meets the large ones
                         // that follow): coarsen the scale first, by an exact power of two, so
@@ -217,11 +260,14 @@ struct Fp64Wavefront {
                             e -= over;
                         }
                     }
-                    const double fM = pow2i(e - eMul);
-                    const double fI = pow2i(e - eIul);
-                    double Mdiag = Mul * fM;
-                    double Idiag = Iul * fI;
-                    double Xdiag = Xul * fI;
+                    double Mdiag = Mul, Idiag = Iul, Xdiag = Xul;
+                    if constexpr (EXT) {
+                        const double fM = pow2i(e - eMul);
+                        const double fI = pow2i(e - eIul);
+                        Mdiag *= fM;
+                        Idiag *= fI;
+                        Xdiag *= fI;
+                    }
 #pragma unroll
                     for (int q = 0; q < Q; ++q) {
                         const double2 lam = trow[q * 32];
@@ -246,23 +292,25 @@ struct Fp64Wavefront {
                     if (writer) {
                         // slot s holds M(s), and X^(s+1), I^(s+1)
                         const int j = k - (G - 1);
-                        if (j >= 0 && j < Hc) { eout[j].m = M[R - 1]; eout[j].e = e; }
-                        if (j >= 1 && j - 1 < Hc) { eout[j - 1].x = Xdiag; eout[j - 1].i = Idiag; eout[j - 1].ei = e; }
+                        if (j >= 0 && j < Hc) border_set_m<EXT>(eout[j], M[R - 1], e);
+                        if (j >= 1 && j - 1 < Hc) border_set_xi<EXT>(eout[j - 1], Xdiag, Idiag, e);
                     }
                     // hand-off: values travel with the sender's exponent
                     Mul = Ml; eMul = eMl;
                     Ml = __shfl_up_sync(kFullMask, M[R - 1], 1, G);
                     Iul = __shfl_up_sync(kFullMask, Idiag, 1, G);
                     Xul = __shfl_up_sync(kFullMask, Xdiag, 1, G);
-                    const int es = __shfl_up_sync(kFullMask, e, 1, G);
-                    eMl = es;
-                    eIul = es;
+                    if constexpr (EXT) {
+                        const int es = __shfl_up_sync(kFullMask, e, 1, G);
+                        eMl = es;
+                        eIul = es;
+                    }
                     if (t == 0) {
                         if (MT && tile > 0) {
                             // the border is indexed by row: it feeds the next step's diagonal
                             if (k < Hc) {
-                                const Border64 b = ring[k & (kRing - 1)];
-                                Mul = b.m; eMul = b.e; Xul = b.x; Iul = b.i; eIul = b.ei;
+                                const Border b = ring[k & (kRing - 1)];
+                                Mul = b.m; eMul = border_e(b); Xul = b.x; Iul = b.i; eIul = border_ei(b);
                             } else {
                                 Mul = 0.0; Xul = 0.0; Iul = 0.0; eMul = 0; eIul = 0;
                             }
@@ -272,7 +320,7 @@ struct Fp64Wavefront {
                     }
                     // renormalise every 16 steps (exact powers of two); a value moves by at
                     // most 2^13 per row, so lanes stay within 2^300 of their scale meanwhile
-                    if ((k & 15) == 15) {
+                    if (EXT && (k & 15) == 15) {
                         // the hand-off values count too: past the read end M is zero and
                         // only the carried I^ and X^ move
                         double mx = fmax(res_lane && k <= kg ? fabs(acc) : 0.0, fmax(fabs(Idiag), fabs(Xdiag)));
@@ -306,6 +354,13 @@ struct Fp64Wavefront {
                 res = log10(acc) - (double)eacc * 0.30102999566398119521 - log10((double)kScale) - log10(beta);
             if (GCP && !(beta > 0.0)) res = NAN;
             v.scores[task.out] = (float)res;
+            // scaled tier: a sum too small (or not finite) for the fixed scale goes on
+            // to the extended tier, which overwrites the score
+            if (!EXT && !(acc >= scaled_tier_threshold(L, H) && acc <= DBL_MAX) && !(GCP && !(beta > 0.0))) {
+                const int cls = fp64_class(L);
+                const unsigned long long slot = atomicAdd(ext.count + cls, 1ull);
+                ext.base[ext.off[cls] + (long long)slot] = task;
+            }
         }
     }
 };

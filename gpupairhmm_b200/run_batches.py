@@ -1,5 +1,10 @@
-"""Run a few batches of one synthetic workload through the engine and print
-the engine's statistics per batch (the command that profiler captures wrap).
+"""Throughput harness: run batches of one synthetic workload through the
+engine and print, per batch, its pairs, cells, FP64 pairs and device stage
+times (packing, FP32 wavefront, FP64 pass) and the call's wall time.  It is
+this package's counterpart of the reference's kernel benchmark
+(benchmark_peakperformance.cu:229-277), on the benchmark configurations'
+shapes instead of uniform lengths, and the command the ncu summaries in
+profiles/ name.
 
   python -m gpupairhmm_b200.run_batches --config uneven --regions 4000 --batches 2
 
@@ -41,7 +46,8 @@ def main() -> None:
         for i in range(a.batches):
             e.compute(inputs)
             s = e.stats()
-            print(f"batch {i}: pairs {s.pairs} cells {s.cells} rescued {s.rescued} device {s.device_ms:.2f} ms "
+            print(f"batch {i}: pairs {s.pairs} cells {s.cells} rescued {s.rescued} (extended {s.rescued_ext}) "
+                  f"device {s.device_ms:.2f} ms "
                   f"(prep {s.prep_ms:.2f}, fp32 {s.fp32_ms:.2f}, fp64 {s.fp64_ms:.2f}) call {s.total_ms:.2f} ms",
                   flush=True)
 

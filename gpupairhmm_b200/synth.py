@@ -230,6 +230,34 @@ def stream_regions(seed: int = 4, rate: float = 2000.0, seconds: float = 60.0, l
         yield t, b.build()
 
 
+def region_pool(seed: int = 4, regions: int = 24000, long_frac: float = 0.05, sigma: float = 1.0) -> list:
+    """cfg4 region shapes drawn ahead of time: `regions` independent regions
+    (config-1 shapes, `long_frac` of them long-read shapes), each a contiguous
+    Batch of one record.  Streams at any rate replay draws from this pool."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(regions):
+        b = _Builder()
+        if rng.random() < long_frac:
+            _cfg3_region(rng, b)
+        else:
+            _cfg1_region(rng, b, sigma)
+        out.append(b.build().contiguous())
+    return out
+
+
+def poisson_arrivals(seed: int, rate: float, seconds: float, pool_size: int):
+    """Poisson arrival times at `rate` per second over `seconds`, each with a
+    region drawn uniformly from a pool of `pool_size`: (times, pool indices)."""
+    rng = np.random.default_rng(seed)
+    n = int(rate * seconds * 1.2 + 100)
+    t = np.cumsum(rng.exponential(1.0 / rate, size=n))
+    while t[-1] < seconds:
+        t = np.concatenate([t, t[-1] + np.cumsum(rng.exponential(1.0 / rate, size=n))])
+    t = t[t <= seconds]
+    return t, rng.integers(0, pool_size, size=len(t))
+
+
 def concat(batches) -> Batch:
     """Records of several batches, in order, as one batch."""
     parts = list(batches)

@@ -27,7 +27,10 @@
  * pairhmm_kernels.cuh:1154).
  *
  * Threading: an engine is used by one host thread at a time (as the
- * reference's worker is).  Different engines are independent.
+ * reference's worker is), except for the serving calls (submit, poll, drain,
+ * region_latency_ms, serving_stats), which may overlap from several threads
+ * (a producer submitting while a consumer drains).  Different engines are
+ * independent.
  */
 #ifndef PAIRHMM_B200_H
 #define PAIRHMM_B200_H
@@ -73,7 +76,10 @@ typedef struct pairhmm_batch {
     const uint8_t* base_quals;
     const uint8_t* ins_quals;
     const uint8_t* del_quals;
-    const uint8_t* gcp_quals;    /* optional, ignored */
+    const uint8_t* gcp_quals;    /* gcp mode (pairhmm_options_t.gcp = 1): required, the first
+                                    position's quality of each read sets its eps and beta;
+                                    default mode: optional and unused, as on the reference's
+                                    GPU path */
     const int64_t* read_offsets; /* [num_reads] */
     const int32_t* read_lengths; /* [num_reads], each >= 1 */
     const uint8_t* hap_bases;
@@ -114,7 +120,7 @@ typedef struct pairhmm_options {
 typedef struct pairhmm_stats {
     int64_t pairs;           /* pairs in the last compute call */
     int64_t cells;           /* sum L*H over those pairs */
-    int64_t rescued;         /* pairs recomputed in FP64 */
+    int64_t rescued;         /* pairs recomputed in FP64 (scaled doubles) */
     int64_t multi_tile_pairs;/* pairs whose read exceeded the largest single tile */
     double device_ms;        /* device time of the last call (CUDA events, launch to scores) */
     double total_ms;         /* host wall time of the last call */
@@ -124,6 +130,9 @@ typedef struct pairhmm_stats {
     int64_t launches;        /* kernels launched by the last call */
     int64_t h2d_bytes;       /* host-to-device bytes copied by the last call */
     int64_t d2h_bytes;       /* device-to-host bytes copied by the last call */
+    int64_t rescued_ext;     /* of those, pairs beyond the scaled doubles' range, recomputed
+                                again with per-lane exponents */
+    int64_t fp32_launches;   /* of launches: the FP32 wavefront launches */
 } pairhmm_stats_t;
 
 typedef struct pairhmm_engine pairhmm_engine_t;
@@ -161,6 +170,22 @@ pairhmm_status_t pairhmm_drain(pairhmm_engine_t* engine, uint64_t ticket, float*
 
 /* Submit-to-completion time of a finished region (valid until it is drained). */
 pairhmm_status_t pairhmm_region_latency_ms(pairhmm_engine_t* engine, uint64_t ticket, double* ms);
+
+/* Admission record of the serving queue (no counterpart in the reference):
+ * regions completed, slot batches run, the most regions and estimated device
+ * bytes admitted into one batch, the admission budget of a slot (device
+ * budget / slots), the slot count, and the most slot batches on the device at
+ * once.  All zero before the first submit. */
+typedef struct pairhmm_serving_stats {
+    int64_t regions;
+    int64_t batches;
+    int64_t max_batch_regions;
+    int64_t max_batch_bytes;
+    int64_t budget_per_slot;
+    int32_t slots;
+    int32_t max_in_flight;
+} pairhmm_serving_stats_t;
+pairhmm_status_t pairhmm_serving_stats(pairhmm_engine_t* engine, pairhmm_serving_stats_t* stats);
 
 /*
  * Tile table: reads of length in (max_len[i-1], max_len[i]] run with groups of
@@ -236,9 +261,14 @@ void pairhmm_set_host_threads(int32_t threads);
  * and every pair's hap_length <= max_hap_length (a longer pair, or an empty
  * read or haplotype, gets NaN); any read length.  FP32 only: pairs whose FP32
  * result underflows are not recomputed in FP64.  The first call on a device
- * sets it up (scratch address, probability table); make that first call
- * before any stream capture.  All calls share the scratch: calls that overlap
- * on the GPU race and must be serialised by the caller.
+ * sets it up (the scratch array's device address, the grid size); make that
+ * first call before any stream capture.  Every call checks the address
+ * against a fresh symbol lookup, so the entry point stays valid after the
+ * device's context is torn down and created again; the probability table is
+ * compiled into the module and needs no upload.  Launch errors are this
+ * call's own: an error the caller left pending is neither returned nor
+ * cleared.  All calls share the scratch: calls that overlap on the GPU race
+ * and must be serialised by the caller.
  */
 typedef struct pairhmm_pair {
     int64_t read_offset;

@@ -31,10 +31,11 @@ _REF = None
 
 
 def build(reference_dir: str | None = None) -> None:
-    """Compile the oracle (and the reference shim when the reference exists)."""
+    """Compile the oracle, and the reference shim when a reference checkout is
+    given (argument or PAIRHMM_REFERENCE_DIR)."""
     subprocess.run(["make", "-s", "-C", str(HERE), "all"], check=True)
-    ref = reference_dir or "/root/reference"
-    if os.path.isdir(ref):
+    ref = reference_dir or os.environ.get("PAIRHMM_REFERENCE_DIR", "")
+    if ref and os.path.isdir(ref):
         subprocess.run(["make", "-s", "-C", str(HERE), "ref", f"REFERENCE_DIR={ref}"], check=True)
 
 

@@ -14,6 +14,7 @@ ref_gpu_<name>.in / ref_gpu_<name>.out
 from __future__ import annotations
 
 import argparse
+import os
 import re
 import subprocess
 import sys
@@ -90,12 +91,13 @@ def ref_gpu(binary: Path, outdir: Path) -> None:
 
 def main() -> None:
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference-dir", default="/root/reference")
+    ap.add_argument("--reference-dir", default=os.environ.get("PAIRHMM_REFERENCE_DIR", ""),
+                    help="reference checkout (default: PAIRHMM_REFERENCE_DIR)")
     ap.add_argument("--ref-gpu", action="store_true", help="run the reference GPU binary (needs a GPU)")
     ap.add_argument("--binary", default=str(ROOT / "oracle" / "_ref" / "gpuPairHMM"))
     ap.add_argument("--outdir", default=str(HERE))
     a = ap.parse_args()
-    if Path(a.reference_dir).is_dir():
+    if a.reference_dir and Path(a.reference_dir).is_dir():
         readme_example(Path(a.reference_dir))
     if a.ref_gpu:
         ref_gpu(Path(a.binary), Path(a.outdir))

@@ -66,6 +66,61 @@ def test_serving_budget_rejects_oversized_region():
     e.close()
 
 
+def test_serving_admission_under_a_small_budget():
+    """A device budget that holds only a few regions per slot batch: a burst of
+    regions is admitted in many budget-limited batches, more than one slot
+    batch is on the device at a time, no batch exceeds its slot's budget, and
+    every region's scores equal the batch call's bitwise."""
+    rng = np.random.default_rng(7)
+    regions = []
+    seed = 500
+    while len(regions) < 48:
+        r = synth.config1(seed=seed, regions=1)
+        seed += 1
+        if int(r.reads_per_record[0]) <= 60:
+            regions.append(r)
+    ref = g.Engine()
+    want = [ref.compute(r) for r in regions]
+    ref.close()
+    e = g.Engine(device_budget_bytes=3 * 400_000)
+    order = rng.permutation(len(regions))
+    tickets = {int(i): e.submit(regions[i]) for i in order}
+    for i, r in enumerate(regions):
+        np.testing.assert_array_equal(e.drain(tickets[i], r.num_pairs, timeout_ms=120000), want[i])
+    st = e.serving_stats()
+    e.close()
+    assert st["regions"] == len(regions)
+    assert st["budget_per_slot"] == 400_000
+    assert 0 < st["max_batch_bytes"] <= st["budget_per_slot"]
+    assert st["batches"] >= 8
+    assert st["max_in_flight"] >= 2
+
+
+def test_serving_concurrent_drains_of_one_ticket():
+    """Two threads drain the same ticket: one gets the scores, the other an
+    unknown-ticket error; nothing else breaks."""
+    e = g.Engine()
+    r = synth.config1(seed=77, regions=1)
+    t = e.submit(r)
+    results = []
+
+    def drain():
+        try:
+            results.append(("ok", e.drain(t, r.num_pairs, timeout_ms=60000)))
+        except g.PairHMMError as err:
+            results.append(("err", err.status))
+
+    ths = [threading.Thread(target=drain) for _ in range(2)]
+    for th in ths:
+        th.start()
+    for th in ths:
+        th.join()
+    kinds = sorted(k for k, _ in results)
+    assert kinds == ["err", "ok"]
+    assert [v for k, v in results if k == "err"] == [5]
+    e.close()
+
+
 def test_cli_end_to_end(tmp_path):
     b = synth.config0(seed=7, records=6)
     text = synth.to_text(b) + synth.to_text(synth.config3(seed=8, regions=1))

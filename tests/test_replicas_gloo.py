@@ -1,7 +1,8 @@
-"""Replicas over several ranks (world_size 2, gloo on CPU): sharding by
-records, per-rank compute, and the gather back into the reference's output
-order.  The per-rank compute here is the oracle (this is a host-logic test);
-on GPUs each rank runs its own engine over the same shard."""
+"""Replicas over several ranks (world_size 2, gloo on CPU) and several
+engines in one process: sharding by records, per-rank compute, and the gather
+back into the reference's output order, through replicas.run_distributed and
+replicas.run.  The per-shard compute here is the oracle (a host-logic test);
+on GPUs the same code runs an engine per device (tests/test_gpu_replicas.py)."""
 import os
 import socket
 
@@ -30,13 +31,16 @@ def _rank_main(rank, world, port, q):
     os.environ["MASTER_PORT"] = str(port)
     dist.init_process_group("gloo", rank=rank, world_size=world)
     b = synth.config1(seed=21, regions=30)
-    part, lo, hi = replicas.shard(b, rank, world)
-    s = oracle.batch_log10(part, nthreads=1).astype(np.float32)
-    assert len(s) == hi - lo
-    parts = [None] * world
-    dist.all_gather_object(parts, (lo, hi, s))
+    seen = []
+
+    def compute(device, part):
+        seen.append((device, part.num_records))
+        return oracle.batch_log10(part, nthreads=1)
+
+    full = replicas.run_distributed(b, device=rank, compute=compute)
+    lo, hi = replicas.shard(b, rank, world)[1:]
+    assert seen == [(rank, replicas.shard(b, rank, world)[0].num_records)] and hi > lo
     if rank == 0:
-        full = replicas.gather(parts, b.num_pairs)
         q.put(full)
     dist.barrier()
     dist.destroy_process_group()
@@ -71,3 +75,29 @@ def test_shard_bounds_cover_and_balance():
         assert sum(per) == cells.sum()
         if world <= 3:
             assert max(per) <= cells.sum() / world + cells.max()
+
+
+def test_in_process_replicas_gather_in_order():
+    """replicas.run with three replicas (the oracle as compute): every shard is
+    computed once, on its own device slot, and the gather gives the one-pass
+    order; a failing replica is reported."""
+    import oracle
+    b = synth.config1(seed=22, regions=25)
+    calls = []
+
+    def compute(device, part):
+        calls.append(device)
+        return oracle.batch_log10(part, nthreads=1)
+
+    full = replicas.run(b, devices=[3, 1, 2], compute=compute)
+    assert sorted(calls) == [1, 2, 3]
+    np.testing.assert_array_equal(full, oracle.batch_log10(b).astype(np.float32))
+
+    def broken(device, part):
+        if device == 1:
+            raise ValueError("device lost")
+        return oracle.batch_log10(part, nthreads=1)
+
+    import pytest
+    with pytest.raises(RuntimeError, match="replica 1"):
+        replicas.run(b, devices=[0, 1], compute=broken)

@@ -102,6 +102,54 @@ def test_noalloc_matches_engine_two_calls():
     assert np.array_equal(got[0], got[1])
 
 
+def test_noalloc_tile_edges_against_oracle():
+    """The allocation-free kernel's own tile and lane residues, checked against
+    the FP64 oracle directly: read lengths at the lane and 512-position tile
+    edges (L - 1 = 15 mod 16 ends a read on a lane's last position), one-base
+    reads and haplotypes, haplotypes of exactly the 16384 limit, on a side
+    stream.  FP32 only: a pair below the FP32 range would be left out of the
+    comparison (this set has none or almost none)."""
+    import torch
+    import gpupairhmm_b200 as g
+    import oracle
+    from gpupairhmm_b200.synth import _Builder
+
+    rng = np.random.default_rng(13)
+    b = _Builder()
+    for L in (1, 16, 17, 511, 512, 513, 1024, 1025):
+        H = np.array([1, 2, L + 40, 16384] if L <= 17 else [L + 40, 2000, 16384])
+        base = ACGT[rng.integers(0, 4, size=16384)]
+        haps = [base[:h].copy() for h in H]
+        reads = []
+        for _ in range(3):  # substrings of the common prefix, 0.3% substitutions
+            s = int(rng.integers(0, 41))
+            r = base[s:s + L].copy()
+            m = rng.random(L) < 0.003
+            r[m] = ACGT[rng.integers(0, 4, size=int(m.sum()))]
+            reads.append(r)
+        n = 3 * L
+        b.add_concat(np.full(3, L), np.concatenate(reads), rng.integers(20, 41, size=n).astype(np.uint8),
+                     rng.integers(30, 46, size=n).astype(np.uint8), rng.integers(30, 46, size=n).astype(np.uint8),
+                     H, np.concatenate(haps))
+    batch = b.build()
+    want = oracle.batch_log10(batch)
+    pairs = pair_list(batch)
+    dev = torch.device("cuda:0")
+    d = [torch.from_numpy(np.ascontiguousarray(getattr(batch, k))).to(dev)
+         for k in ("read_bases", "base_quals", "ins_quals", "del_quals", "hap_bases")]
+    dpairs = torch.from_numpy(pairs.view(np.uint8)).to(dev)
+    scores = torch.full((len(pairs),), float("nan"), dtype=torch.float32, device=dev)
+    side = torch.cuda.Stream(dev)
+    side.wait_stream(torch.cuda.current_stream(dev))
+    with torch.cuda.stream(side):
+        g.forward_pairs_noalloc(0, *d, dpairs, len(pairs), 16384, scores, side)
+    side.synchronize()
+    got = scores.cpu().numpy()
+    ok = want > -60.0
+    assert ok.sum() >= 0.9 * len(want)
+    assert_log10_close(got[ok], want[ok], RTOL, ATOL, what="no-alloc tile edges vs oracle")
+
+
 def test_noalloc_limits():
     import torch
     import gpupairhmm_b200 as g
