@@ -123,6 +123,7 @@ _SIGNATURES = {
     "pairhmm_set_tile_table": (ctypes.c_int, [_P, _P, _P, _P, _P, ctypes.c_int32]),
     "pairhmm_get_tile_table": (ctypes.c_int, [_P, _P, _P, _P, _P, ctypes.c_int32, _P]),
     "pairhmm_probe_fp32_peak": (ctypes.c_int, [ctypes.c_int32, ctypes.c_int32, _P]),
+    "pairhmm_probe_fp64_peak": (ctypes.c_int, [ctypes.c_int32, ctypes.c_int32, _P]),
     "pairhmm_status_string": (ctypes.c_char_p, [ctypes.c_int]),
     "pairhmm_last_error": (ctypes.c_char_p, [_P]),
     "pairhmm_batch_counts": (ctypes.c_int, [_P, _P, _P]),
@@ -398,6 +399,13 @@ def probe_fp32_peak(device: int = 0, milliseconds: int = 50) -> float:
     """Measured FP32 FMA throughput in TFLOP/s (2 FLOP per FMA)."""
     v = ctypes.c_double()
     _check(lib().pairhmm_probe_fp32_peak(device, milliseconds, ctypes.byref(v)))
+    return float(v.value)
+
+
+def probe_fp64_peak(device: int = 0, milliseconds: int = 50) -> float:
+    """Measured FP64 FMA throughput in TFLOP/s (2 FLOP per FMA)."""
+    v = ctypes.c_double()
+    _check(lib().pairhmm_probe_fp64_peak(device, milliseconds, ctypes.byref(v)))
     return float(v.value)
 
 

@@ -364,7 +364,13 @@ pairhmm_status_t pairhmm_get_tile_table(pairhmm_engine_t* h, int32_t* max_len, i
     return PAIRHMM_OK;
 }
 
-pairhmm_status_t pairhmm_probe_fp32_peak(int32_t device, int32_t milliseconds, double* tflops) {
+}  // extern "C"
+
+namespace {
+// FMA throughput of one of the probe kernels: grow the launch until it takes
+// the requested time, keep the best rate
+pairhmm_status_t probe_peak(int32_t device, int32_t milliseconds, double* tflops,
+                            cudaError_t (*launch)(float*, int, int, cudaStream_t)) {
     if (!tflops || milliseconds <= 0) return PAIRHMM_ERR_INVALID_ARGUMENT;
     if (cudaSetDevice(device) != cudaSuccess) return PAIRHMM_ERR_CUDA;
     cudaDeviceProp prop{};
@@ -383,7 +389,7 @@ pairhmm_status_t pairhmm_probe_fp32_peak(int32_t device, int32_t milliseconds, d
     // grow until one launch takes the requested time, then keep the best of 3
     for (int rep = 0; rep < 12 && st == PAIRHMM_OK; ++rep) {
         cudaEventRecord(a, s);
-        if (phmm::launch_ffma_peak(out, grid, iters, s) != cudaSuccess) st = PAIRHMM_ERR_CUDA;
+        if (launch(out, grid, iters, s) != cudaSuccess) st = PAIRHMM_ERR_CUDA;
         cudaEventRecord(b, s);
         if (cudaEventSynchronize(b) != cudaSuccess) st = PAIRHMM_ERR_CUDA;
         float ms = 0.f;
@@ -398,6 +404,17 @@ pairhmm_status_t pairhmm_probe_fp32_peak(int32_t device, int32_t milliseconds, d
     cudaStreamDestroy(s);
     cudaFree(out);
     return st;
+}
+}  // namespace
+
+extern "C" {
+
+pairhmm_status_t pairhmm_probe_fp32_peak(int32_t device, int32_t milliseconds, double* tflops) {
+    return probe_peak(device, milliseconds, tflops, &phmm::launch_ffma_peak);
+}
+
+pairhmm_status_t pairhmm_probe_fp64_peak(int32_t device, int32_t milliseconds, double* tflops) {
+    return probe_peak(device, milliseconds, tflops, &phmm::launch_dfma_peak);
 }
 
 }  // extern "C"

@@ -83,5 +83,7 @@ cudaError_t launch_binning(BinArgs a, int grid, cudaStream_t s, const int* per_t
 // FP32 FFMA throughput probe used to measure the roofline denominator:
 // `iters` dependent-chain-free FMAs per thread over grid x 256 threads.
 cudaError_t launch_ffma_peak(float* out, int grid, int iters, cudaStream_t s);
+// The same with double FMAs.
+cudaError_t launch_dfma_peak(float* out, int grid, int iters, cudaStream_t s);
 
 }  // namespace phmm

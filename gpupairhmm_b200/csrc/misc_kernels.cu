@@ -214,4 +214,25 @@ cudaError_t launch_ffma_peak(float* out, int grid, int iters, cudaStream_t s) {
     return cudaGetLastError();
 }
 
+// The same with double FMAs (the FP64 pass's roofline denominator).
+__global__ void __launch_bounds__(256) dfma_peak_kernel(float* out, int iters) {
+    double a0 = threadIdx.x * 1e-3, a1 = a0 + 1.0, a2 = a0 + 2.0, a3 = a0 + 3.0;
+    double a4 = a0 + 4.0, a5 = a0 + 5.0, a6 = a0 + 6.0, a7 = a0 + 7.0;
+    const double b = 0.9999, c = 1e-7;
+    for (int i = 0; i < iters; ++i) {
+#pragma unroll
+        for (int u = 0; u < 16; ++u) {
+            a0 = fma(a0, b, c); a1 = fma(a1, b, c); a2 = fma(a2, b, c); a3 = fma(a3, b, c);
+            a4 = fma(a4, b, c); a5 = fma(a5, b, c); a6 = fma(a6, b, c); a7 = fma(a7, b, c);
+        }
+    }
+    const double s = a0 + a1 + a2 + a3 + a4 + a5 + a6 + a7;
+    if (s == 12345.678) out[0] = (float)s;  // keeps the chains live
+}
+
+cudaError_t launch_dfma_peak(float* out, int grid, int iters, cudaStream_t s) {
+    dfma_peak_kernel<<<grid, 256, 0, s>>>(out, iters);
+    return cudaGetLastError();
+}
+
 }  // namespace phmm

@@ -94,7 +94,7 @@ forward_pairs_kernel(const uint8_t* __restrict__ read_bases, const uint8_t* __re
         const uint8_t* hb = hap_bases + pr.hap_offset;
         const int ntiles = (L + kT - 1) / kT;
         const float Dbound = kBeta * (kScale / (float)H);
-        float acc = 0.f;
+        double acc = 0.0;  // summed in double: up to 16384 rows of similar size
         int rlane = -1;
         for (int tile = 0; tile < ntiles; ++tile) {  // (pair loop strides by nwarps)
             const bool last = tile == ntiles - 1;
@@ -152,8 +152,9 @@ forward_pairs_kernel(const uint8_t* __restrict__ read_bases, const uint8_t* __re
                     Xdiag = In + Dold;
                 }
                 if (res_lane) {
-                    acc += Idiag;
-                    if (addM && k < kg) acc = fmaf(kBeta, M[kR - 1], acc);
+                    float a = Idiag;
+                    if (addM && k < kg) a = fmaf(kBeta, M[kR - 1], a);
+                    acc += (double)a;
                 }
                 if (writer) {
                     const int j = k - (kG - 1);
@@ -187,7 +188,7 @@ forward_pairs_kernel(const uint8_t* __restrict__ read_bases, const uint8_t* __re
             }
             __syncwarp();
         }
-        if (t == rlane) scores[pi] = log10f(acc) - (log10f(kScale) + log10f(kBeta));
+        if (t == rlane) scores[pi] = (float)(log10(acc) - (log10((double)kScale) + log10((double)kBeta)));
     }
 }
 

@@ -39,7 +39,10 @@
 // carry); beta times the lane's last I^ is then beta*(M+I)(j, L-1) (the
 // reference's trick, pairhmm_kernels.cuh:1307-1331, with beta folded in).
 // When the read ends on a lane's last position the lane adds q*I^ + beta*N.
-// Summing over j gives beta * sum_j (M+I)(L-1,j).
+// Summing over j gives beta * sum_j (M+I)(L-1,j).  The sum runs over up to
+// H rows of similar size, which in FP32 alone drifts by up to ~H*2^-25
+// relative (1e-4 at H = 16384); each block of 4 steps is summed in FP32 and
+// the blocks in double, so it is exact to well below the output's precision.
 //
 // lam' table: each thread owns 5 x R floats in shared memory, laid out as
 // [hap code][R/4][32 lanes] float4, so a warp-wide 16-byte load touches 32
@@ -56,6 +59,16 @@
 // i writes (X^, I^, N) of its last position for every haplotype row into a
 // per-group scratch border, which lane 0 of tile i+1 reads as its left
 // boundary (pairhmm_kernels.cuh:2167-3272 does the same with 512-row tiles).
+//
+// Early hand-off of long pairs that will underflow: every path to the result
+// crosses the border column once, and transitions and emissions never exceed
+// 1, so the final sum is at most the mass on the border, sum_j (M+I+D)(j).
+// After each tile but the last the group adds up its border rows (in L2, a
+// few loads per lane); when that mass is below half the FP64 threshold the
+// final sum would be below the threshold too, so the pair is flagged for the
+// FP64 pass at once and its remaining tiles are skipped.  Which pairs the
+// FP64 pass recomputes, and so every result, is unchanged; long unrelated
+// reads no longer run their later FP32 tiles for nothing.
 #pragma once
 
 #include "device_common.cuh"
@@ -127,13 +140,14 @@ struct Fp32Wavefront {
         const float beta = GCP ? (float)(1.0 - (double)eps) : kBeta;
         const float Dbound = beta * (kScale / (float)Hc);
 
-        float acc = 0.f;
+        double accd = 0.0;       // result sum: 4-step FP32 blocks added in double
         int rlane = -1;          // lane (in group) that holds the result
         bool degenerate = false; // some |alpha| < kMinAlpha: FP64 pass recomputes the pair
         if (GCP && !(beta >= kMinAlpha)) degenerate = true;  // gcp quality 0: nothing to rescale by
 
+        bool handed_off = false;  // MT: flagged for the FP64 pass at a tile border
         for (int tile = 0; tile < nt_warp; ++tile) {
-            const bool tile_live = valid && tile < ntiles;
+            const bool tile_live = valid && !handed_off && tile < ntiles;
             const bool last = tile == ntiles - 1;
             const int p0 = tile * T + t * R;
 
@@ -252,6 +266,7 @@ struct Fp32Wavefront {
                 eout = gbase + (tile & 1) * rows;
             }
             const bool writer = MT && tile_live && !last && t == G - 1;
+            float ib0 = 0.f;  // writer: I^ of row 0 on the border column
 
             // code words of this group's haplotype; a group whose haplotype is
             // shorter than the warp's step count keeps re-reading its last word
@@ -261,6 +276,7 @@ struct Fp32Wavefront {
             uint32_t wnext = __ldg(hw + 1);
             for (int k0 = 0; k0 < K; k0 += 4) {
                 const uint32_t wpref = __ldg(hw + min_i((k0 >> 2) + 2, wlast));
+                float acc = 0.f;
 #pragma unroll
                 for (int s = 0; s < 4; ++s) {
                     const int k = k0 + s;
@@ -300,8 +316,9 @@ struct Fp32Wavefront {
                         if (addM && k < kg) acc = fmaf(beta, N[R - 1], acc);
                     }
                     if (MT && writer) {
-                        // slot s holds X^(s+1), I^(s+1), N(s)
+                        // slot s holds X^(s+1), I^(s+1), N(s); I^(0) stays in a register
                         const int j = k - (G - 1);
+                        if (j == 0) ib0 = Idiag;
                         if (j >= 0 && j < Hc) reinterpret_cast<float*>(eout + j)[2] = N[R - 1];
                         if (j >= 1 && j - 1 < Hc)
                             *reinterpret_cast<float2*>(eout + (j - 1)) = make_float2(Xdiag, Idiag);
@@ -330,20 +347,49 @@ struct Fp32Wavefront {
                         Xul = Dbound;
                     }
                 }
+                if (res_lane) accd += (double)acc;
                 wcur = wnext;
                 wnext = wpref;
             }
             __syncwarp();
+            const bool check = MT && v.rescue_enabled && tile_live && !last;
+            if (MT && __any_sync(kFullMask, check)) {  // warp-uniform: every lane shuffles
+                // mass on this tile's border column: slot s holds X^(s+1), I^(s+1), N(s);
+                // M = N/alpha_next, I + D(j-1) = q*X^/beta and I(0) = q*I^(0)/beta at the
+                // last position of lane G-1 (the sum also takes I of the row after the
+                // haplotype's last, which only makes it larger)
+                const int src = grp * G + G - 1;
+                const float an = __shfl_sync(kFullMask, alpha_next, src);
+                const float qb = __shfl_sync(kFullMask, q_last, src) / beta;
+                const float i0 = __shfl_sync(kFullMask, ib0, src);
+                float mass = 0.f;
+                if (check) {
+                    if (t == 0) mass = qb * i0;
+                    for (int j = t; j < Hc; j += G) {
+                        const float4 b = __ldcg(eout + j);
+                        mass += b.z / an + qb * b.x;
+                    }
+                }
+#pragma unroll
+                for (int d = G / 2; d >= 1; d >>= 1) mass += __shfl_xor_sync(kFullMask, mass, d, G);
+                if (check && mass < 0.5f * rescue_threshold(L, H)) handed_off = true;
+            }
+            if (MT && __all_sync(kFullMask, !valid || handed_off || tile + 1 >= ntiles)) break;
         }
 
         // any lane of the group saw a degenerate alpha
         const unsigned dmask = __ballot_sync(kFullMask, degenerate);
         const unsigned gmask = (G == 32 ? kFullMask : ((1u << G) - 1u)) << (grp * G);
         degenerate = (dmask & gmask) != 0u;
-        if (valid && t == rlane) {
-            const float res = log10f(acc) - (log10f(kScale) + log10f(beta));
+        if (valid && handed_off && t == 0) {
+            v.scores[task.out] = -INFINITY;  // the FP64 pass writes the result
+            append_rescue(v, fp64_class(L), task);
+        }
+        if (valid && !handed_off && t == rlane) {
+            const float res = (float)(log10(accd) - (log10((double)kScale) + log10((double)beta)));
             v.scores[task.out] = res;
-            if (degenerate || (v.rescue_enabled && !(acc >= rescue_threshold(L, H) && acc <= FLT_MAX))) {
+            if (degenerate ||
+                (v.rescue_enabled && !(accd >= (double)rescue_threshold(L, H) && accd <= (double)FLT_MAX))) {
                 append_rescue(v, fp64_class(L), task);
             }
         }

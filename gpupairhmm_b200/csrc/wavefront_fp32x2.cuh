@@ -156,7 +156,7 @@ struct Fp32x2Wavefront {
         const float2 k01 = f2(kEps, kEps);
         float2 Ml = f2(0.f, 0.f), Mul = Ml, Iul = Ml, Xul = Ml;
         if (t == 0) Xul = f2(Dbound, Dbound);
-        float accA = 0.f, accB = 0.f;
+        double accdA = 0.0, accdB = 0.0;  // result sums: 4-step FP32 blocks added in double
         int h = 4;
 
         const int wlast = ((Hc + 15) & ~15) / 4 - 1;
@@ -164,6 +164,7 @@ struct Fp32x2Wavefront {
         uint32_t wnext = __ldg(hw + 1);
         for (int k0 = 0; k0 < K; k0 += 4) {
             const uint32_t wpref = __ldg(hw + min_i((k0 >> 2) + 2, wlast));
+            float accA = 0.f, accB = 0.f;
 #pragma unroll
             for (int s = 0; s < 4; ++s) {
                 const int k = k0 + s;
@@ -207,6 +208,8 @@ struct Fp32x2Wavefront {
                     Xul = f2(Dbound, Dbound);
                 }
             }
+            if (resA) accdA += (double)accA;
+            if (resB) accdB += (double)accB;
             wcur = wnext;
             wnext = wpref;
         }
@@ -215,16 +218,16 @@ struct Fp32x2Wavefront {
         const unsigned gmask = (G == 32 ? kFullMask : ((1u << G) - 1u)) << (grp * G);
         degA = (__ballot_sync(kFullMask, degA) & gmask) != 0u;
         degB = (__ballot_sync(kFullMask, degB) & gmask) != 0u;
-        const float off = log10f(kScale) + log10f(kBeta);
+        const double off = log10((double)kScale) + log10((double)kBeta);
         if (resA) {
-            v.scores[it.out0] = log10f(accA) - off;
-            if (degA || (v.rescue_enabled && !(accA >= rescue_threshold(LA, H) && accA <= FLT_MAX))) {
+            v.scores[it.out0] = (float)(log10(accdA) - off);
+            if (degA || (v.rescue_enabled && !(accdA >= (double)rescue_threshold(LA, H) && accdA <= (double)FLT_MAX))) {
                 append_rescue(v, fp64_class(LA), Task{ra, it.hap, it.out0});
             }
         }
         if (resB) {
-            v.scores[it.out1] = log10f(accB) - off;
-            if (degB || (v.rescue_enabled && !(accB >= rescue_threshold(LB, H) && accB <= FLT_MAX))) {
+            v.scores[it.out1] = (float)(log10(accdB) - off);
+            if (degB || (v.rescue_enabled && !(accdB >= (double)rescue_threshold(LB, H) && accdB <= (double)FLT_MAX))) {
                 append_rescue(v, fp64_class(LB), Task{rb, it.hap, it.out1});
             }
         }

@@ -207,6 +207,8 @@ pairhmm_status_t pairhmm_get_tile_table(pairhmm_engine_t* engine, int32_t* max_l
  * of `device` in TFLOP/s (2 FLOP per FMA), best of several launches of about
  * `milliseconds` each.  Used as the roofline denominator. */
 pairhmm_status_t pairhmm_probe_fp32_peak(int32_t device, int32_t milliseconds, double* tflops);
+/* The same for FP64 FMAs: the FP64 pass's roofline denominator. */
+pairhmm_status_t pairhmm_probe_fp64_peak(int32_t device, int32_t milliseconds, double* tflops);
 
 /*
  * Record file format (README.md:41-61).  A parsed buffer owns its arrays; the

@@ -98,6 +98,24 @@ def test_haplotype_length_sweep(engine):
     assert_log10_close(engine.compute(b), oracle.batch_log10(b), what="hap sweep")
 
 
+def test_result_sum_over_long_haplotypes(engine, plain_engine):
+    """Short reads on haplotypes of 5,000 and 16,384 positions: the result is a
+    sum of thousands of rows of similar size and lies near zero, where the
+    tolerance is tightest (1e-5 relative of a log10 near -1); every kernel form
+    (scalar, packed, plain) must sum it without drift."""
+    rng = np.random.default_rng(71)
+    recs = [_record(rng, L, H, n_reads=3, n_haps=2) for L in (1, 2, 5, 16, 33, 100) for H in (5000, 16384)]
+    b = _soa(recs)
+    want = oracle.batch_log10(b)
+    assert_log10_close(engine.compute(b), want, what="long haplotype sums, engine")
+    ok = want > -60.0  # the plain form is FP32 only
+    assert_log10_close(plain_engine.compute(b)[ok], want[ok], what="long haplotype sums, plain")
+    e = g.Engine()
+    e.set_tile_table(PACKED_TABLE)
+    assert_log10_close(e.compute(b), want, what="long haplotype sums, packed")
+    e.close()
+
+
 def test_n_lowercase_and_odd_letters(engine):
     rng = np.random.default_rng(8)
     recs = [_record(rng, L, H, letters="ACGTNacgtX") for L, H in [(7, 9), (64, 80), (150, 300), (250, 260)]]
