@@ -252,18 +252,23 @@ struct Fp32Wavefront {
             if (t == 0 && tile == 0) Xul = Dbound;
             int h = 4;
 
-            // border in/out (MT only)
+            // border in/out (MT only).  Row j of a buffer sits at entry G + j: the last
+            // lane writes rows k - G .. k - G + 1 at step k from k = 0 on without bounds
+            // branches, rows before 0 and after the haplotype's last landing in the
+            // padding (a buffer has at least max H + 72 entries; a tile's last write is
+            // row H + 3, at entry H + G + 3)
             float4* ein = nullptr;
             float4* eout = nullptr;
+            const int64_t nrow = rows - G;  // rows a buffer holds after the padding
             float4 bcur = make_float4(0.f, 0.f, 0.f, 0.f), bnext = bcur;
             if (MT) {
                 float4* gbase = scratch + (int64_t)grp * 2 * rows;
                 if (tile > 0) {
-                    ein = gbase + ((tile - 1) & 1) * rows;
-                    if (t < rows) bcur = __ldcg(ein + t);
-                    if (G + t < rows) bnext = __ldcg(ein + G + t);
+                    ein = gbase + ((tile - 1) & 1) * rows + G;
+                    if (t < nrow) bcur = __ldcg(ein + t);
+                    if (G + t < nrow) bnext = __ldcg(ein + G + t);
                 }
-                eout = gbase + (tile & 1) * rows;
+                eout = gbase + (tile & 1) * rows + G;
             }
             const bool writer = MT && tile_live && !last && t == G - 1;
             float ib0 = 0.f;  // writer: I^ of row 0 on the border column
@@ -319,9 +324,8 @@ struct Fp32Wavefront {
                         // slot s holds X^(s+1), I^(s+1), N(s); I^(0) stays in a register
                         const int j = k - (G - 1);
                         if (j == 0) ib0 = Idiag;
-                        if (j >= 0 && j < Hc) reinterpret_cast<float*>(eout + j)[2] = N[R - 1];
-                        if (j >= 1 && j - 1 < Hc)
-                            *reinterpret_cast<float2*>(eout + (j - 1)) = make_float2(Xdiag, Idiag);
+                        reinterpret_cast<float*>(eout + j)[2] = N[R - 1];
+                        *reinterpret_cast<float2*>(eout + (j - 1)) = make_float2(Xdiag, Idiag);
                     }
                     // boundary hand-off
                     Mul = Ml;
@@ -339,7 +343,7 @@ struct Fp32Wavefront {
                         if (src == G - 1) {
                             bcur = bnext;
                             const int64_t idx = (int64_t)k + 1 + G + t;
-                            bnext = idx < rows ? __ldcg(ein + idx) : make_float4(0.f, 0.f, 0.f, 0.f);
+                            bnext = idx < nrow ? __ldcg(ein + idx) : make_float4(0.f, 0.f, 0.f, 0.f);
                         }
                     } else if (t == 0) {
                         Ml = 0.f;

@@ -105,6 +105,11 @@ struct Fp64Wavefront {
     static constexpr int Q = R / 2;                   // double2 per thread per table row
     static constexpr int kTableDouble2 = 5 * Q * 32;  // per warp
     static constexpr int kRing = 32;
+    // border rows sit kRowPad entries into the warp's buffer: the last lane writes row
+    // k - (G - 1) at step k from k = 0 on, without bounds branches (rows before 0 and
+    // after the haplotype's last fall in the padding; the buffer has at least
+    // max H + 72 rows, and the last write of a tile is row H + 4)
+    static constexpr int kRowPad = G;
     using Border = typename std::conditional<EXT, Border64, Border64S>::type;
     // largest scale difference a hand-off converts: stored values stay within
     // about 2^(64 + 13*16) of 1 between renormalisations, so 2^640 more keeps
@@ -213,7 +218,7 @@ struct Fp64Wavefront {
             Border* eout = scratch;
             const bool writer = MT && valid && !last && t == G - 1;
             Border nb{};
-            if (MT && tile > 0 && t < rows) nb = ein[t];
+            if (MT && tile > 0 && t + kRowPad < rows) nb = ein[t + kRowPad];
             int h = 4;
 
             // code words of this group's haplotype, clamped to its own extent
@@ -227,7 +232,7 @@ struct Fp64Wavefront {
                     ring[t] = nb;
                     __syncwarp();
                     const int64_t idx = (int64_t)k0 + kRing + t;
-                    if (idx < rows) nb = ein[idx];
+                    if (idx + kRowPad < rows) nb = ein[idx + kRowPad];
                 }
 #pragma unroll
                 for (int s = 0; s < 4; ++s) {
@@ -290,10 +295,11 @@ struct Fp64Wavefront {
                         if (addM && k < kg) acc = fma(beta, M[R - 1], acc);
                     }
                     if (writer) {
-                        // slot s holds M(s), and X^(s+1), I^(s+1)
+                        // slot s + kRowPad holds M(s), and X^(s+1), I^(s+1); rows before the
+                        // haplotype and past it land in the padding and are never read
                         const int j = k - (G - 1);
-                        if (j >= 0 && j < Hc) border_set_m<EXT>(eout[j], M[R - 1], e);
-                        if (j >= 1 && j - 1 < Hc) border_set_xi<EXT>(eout[j - 1], Xdiag, Idiag, e);
+                        border_set_m<EXT>(eout[j + kRowPad], M[R - 1], e);
+                        border_set_xi<EXT>(eout[j - 1 + kRowPad], Xdiag, Idiag, e);
                     }
                     // hand-off: values travel with the sender's exponent
                     Mul = Ml; eMul = eMl;
@@ -305,18 +311,17 @@ struct Fp64Wavefront {
                         eMl = es;
                         eIul = es;
                     }
-                    if (t == 0) {
-                        if (MT && tile > 0) {
-                            // the border is indexed by row: it feeds the next step's diagonal
-                            if (k < Hc) {
-                                const Border b = ring[k & (kRing - 1)];
-                                Mul = b.m; eMul = border_e(b); Xul = b.x; Iul = b.i; eIul = border_ei(b);
-                            } else {
-                                Mul = 0.0; Xul = 0.0; Iul = 0.0; eMul = 0; eIul = 0;
-                            }
-                        } else {
-                            Ml = 0.0; Iul = 0.0; Xul = Dbound; eMl = 0; eIul = 0;
+                    if (MT && tile > 0) {
+                        // the border is indexed by row: it feeds the next step's diagonal;
+                        // every lane takes part in the (broadcast) load, lane 0 keeps it
+                        const Border b = ring[k & (kRing - 1)];
+                        if (t == 0) {
+                            const bool in = k < Hc;
+                            Mul = in ? b.m : 0.0; Xul = in ? b.x : 0.0; Iul = in ? b.i : 0.0;
+                            eMul = in ? border_e(b) : 0; eIul = in ? border_ei(b) : 0;
                         }
+                    } else if (t == 0) {
+                        Ml = 0.0; Iul = 0.0; Xul = Dbound; eMl = 0; eIul = 0;
                     }
                     // renormalise every 16 steps (exact powers of two); a value moves by at
                     // most 2^13 per row, so lanes stay within 2^300 of their scale meanwhile
