@@ -36,7 +36,7 @@ SINGLE = [(G, R) for G in (4, 8, 16, 32) for R in (4, 8, 12, 16, 20, 24, 28, 32)
 # tiles with R % 4 == 2 where G*R falls on a class bound that no other tile has
 SINGLE += [(8, 14), (8, 18), (8, 22), (16, 10), (16, 14), (16, 18)]
 MULTI = [(32, 16), (32, 20), (32, 24), (32, 28), (32, 32), (16, 32)]
-PACKED = [(G, R) for G in (4, 8, 16, 32) for R in (8, 12, 16)]  # two reads per group, packed FP32
+PACKED = [(G, R) for G in (4, 8, 16, 32) for R in (8, 12, 16)] + [(16, 10)]  # two reads per group, packed FP32
 
 
 def classes():

@@ -13,6 +13,7 @@ void register_fp32_g16(std::vector<ConfigInfo>& out) {
     out.push_back(make_fp32_config<16, 32, false>());
     out.push_back(make_fp32_config<16, 32, true>());
     out.push_back(make_fp32_config<16, 8, false, true>());
+    out.push_back(make_fp32_config<16, 10, false, true>());
     out.push_back(make_fp32_config<16, 12, false, true>());
     out.push_back(make_fp32_config<16, 16, false, true>());
 }

@@ -21,7 +21,7 @@ using WavefrontOf = typename std::conditional<PK, Fp32x2Wavefront<G, R>, Fp32Wav
 // natural allocation sits just above an occupancy step (64-thread CTAs: 6 CTAs
 // at <= 170 registers); 1 leaves the allocator free.
 constexpr int fp32_min_ctas(int R, bool MT, bool PK) {
-    return PK ? (R <= 8 ? 6 : 1) : (!MT && R <= 20 ? 6 : 1);
+    return PK ? (R <= 10 ? 6 : 1) : (!MT && R <= 20 ? 6 : 1);
 }
 
 template <int G, int R, bool MT, bool PK, bool GCP = false>

@@ -22,23 +22,45 @@ __device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b
 
 template <int G, int R>
 struct Fp32x2Wavefront {
-    static_assert(R % 4 == 0 && R >= 4, "R must be a multiple of 4");
+    static_assert(R % 2 == 0 && R >= 4, "R must be even");
     static_assert(G == 4 || G == 8 || G == 16 || G == 32, "G must divide the warp");
     static constexpr int NG = 32 / G;   // items (pairs of pairs) per warp
     static constexpr int T = G * R;
     static constexpr int Q = R / 2;     // float4 (2 positions x 2 reads) per thread per table row
     static constexpr int kTableFloat4 = 5 * Q * 32;  // per warp
+    // read positions in groups of 4, the last group 2 when R % 4 == 2 (a lane then
+    // starts 8-byte aligned and loads its packed words as uint2 pairs)
+    static constexpr int NGRP = R / 4 + (R % 4 ? 1 : 0);
+    __host__ __device__ static constexpr int group_size(int g) { return g < R / 4 ? 4 : 2; }
+
+    __device__ __forceinline__ static void load_group(const uint32_t* rpack, int p0, int g, int L, uint32_t (&ws)[4]) {
+        ws[0] = ws[1] = ws[2] = ws[3] = 0u;
+        const int p = p0 + 4 * g;
+        if (p >= L) return;
+        if (g < R / 4) {
+            if constexpr (R % 4 == 0) {
+                const uint4 w = __ldg(reinterpret_cast<const uint4*>(rpack + p));
+                ws[0] = w.x; ws[1] = w.y; ws[2] = w.z; ws[3] = w.w;
+            } else {
+                const uint2 a = __ldg(reinterpret_cast<const uint2*>(rpack + p));
+                const uint2 b = __ldg(reinterpret_cast<const uint2*>(rpack + p + 2));
+                ws[0] = a.x; ws[1] = a.y; ws[2] = b.x; ws[3] = b.y;
+            }
+        } else {
+            const uint2 a = __ldg(reinterpret_cast<const uint2*>(rpack + p));
+            ws[0] = a.x; ws[1] = a.y;
+        }
+    }
 
     __device__ __forceinline__ static void params(const DevView& v, const uint32_t* rpack, int L, int p0, const float* ph,
                                   float (&a_cur)[R], float& a_next) {
 #pragma unroll
-        for (int q = 0; q < R / 4; ++q) {
-            uint4 w = make_uint4(0u, 0u, 0u, 0u);
-            if (p0 + 4 * q < L) w = __ldg(reinterpret_cast<const uint4*>(rpack + p0 + 4 * q));
-            const uint32_t ws[4] = {w.x, w.y, w.z, w.w};
+        for (int g = 0; g < NGRP; ++g) {
+            uint32_t ws[4];
+            load_group(rpack, p0, g, L, ws);
 #pragma unroll
-            for (int s = 0; s < 4; ++s) {
-                const int r = 4 * q + s;
+            for (int s = 0; s < group_size(g); ++s) {
+                const int r = 4 * g + s;
                 a_cur[r] = (p0 + r < L) ? 1.0f - (ph[(ws[s] >> 16) & 0x7fu] + ph[(ws[s] >> 24) & 0x7fu]) : 1.0f;
             }
         }
@@ -109,15 +131,13 @@ struct Fp32x2Wavefront {
         float2 dpv[R], ee[R], rr[R], N[R], D[R];
         float qpA = scale_before(rpA, LAc, p0, ph), qpB = scale_before(rpB, LBc, p0, ph);
 #pragma unroll
-        for (int q = 0; q < R / 4; ++q) {
-            uint4 wa = make_uint4(0u, 0u, 0u, 0u), wb = wa;
-            if (p0 + 4 * q < LAc) wa = __ldg(reinterpret_cast<const uint4*>(rpA + p0 + 4 * q));
-            if (p0 + 4 * q < LBc) wb = __ldg(reinterpret_cast<const uint4*>(rpB + p0 + 4 * q));
-            const uint32_t was[4] = {wa.x, wa.y, wa.z, wa.w};
-            const uint32_t wbs[4] = {wb.x, wb.y, wb.z, wb.w};
+        for (int q = 0; q < NGRP; ++q) {
+            uint32_t was[4], wbs[4];
+            load_group(rpA, p0, q, LAc, was);
+            load_group(rpB, p0, q, LBc, wbs);
             float lamA[5][4], lamB[5][4];
 #pragma unroll
-            for (int s = 0; s < 4; ++s) {
+            for (int s = 0; s < group_size(q); ++s) {
                 const int r = 4 * q + s;
                 const int c = p0 + r;
                 const float anA_r = (r + 1 < R) ? aA[r + 1 < R ? r + 1 : r] : anA;
@@ -136,7 +156,9 @@ struct Fp32x2Wavefront {
 #pragma unroll
             for (int hh = 0; hh < 5; ++hh) {
                 wtab[(hh * Q + 2 * q) * 32 + lane] = make_float4(lamA[hh][0], lamB[hh][0], lamA[hh][1], lamB[hh][1]);
-                wtab[(hh * Q + 2 * q + 1) * 32 + lane] = make_float4(lamA[hh][2], lamB[hh][2], lamA[hh][3], lamB[hh][3]);
+                if (group_size(q) == 4)
+                    wtab[(hh * Q + 2 * q + 1) * 32 + lane] =
+                        make_float4(lamA[hh][2], lamB[hh][2], lamA[hh][3], lamB[hh][3]);
             }
         }
 

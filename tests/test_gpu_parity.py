@@ -90,6 +90,22 @@ def test_even_r_tiles_match_oracle(G, R):
     assert_log10_close(got, oracle.batch_log10(b), what=f"{G}x{R} tile")
 
 
+def test_packed_even_r_tile_matches_oracle():
+    """The packed kernel with R % 4 == 2 (16 x 10, lanes 8-byte aligned, the last
+    two positions of a lane in their own table entry): read lengths at every lane
+    and tile edge, records with odd read counts (one-read units)."""
+    rng = np.random.default_rng(61)
+    lens = sorted({1, 2, 3, 8, 9, 10, 11, 12, 19, 20, 21, 79, 80, 81, 129, 144, 150, 158, 159, 160})
+    recs = [_record(rng, L, int(rng.integers(max(L, 8), L + 300)), n_reads=1 + i % 3, n_haps=2)
+            for i, L in enumerate(lens)]
+    b = _soa(recs)
+    e = g.Engine()
+    e.set_tile_table([(160, 16, 10, 2), (1 << 30, 32, 32, 1)])
+    got = e.compute(b)
+    e.close()
+    assert_log10_close(got, oracle.batch_log10(b), what="packed 16x10 tile")
+
+
 def test_haplotype_length_sweep(engine):
     rng = np.random.default_rng(6)
     recs = [_record(rng, 100, H, n_reads=3, n_haps=2) for H in
