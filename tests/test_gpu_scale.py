@@ -81,3 +81,36 @@ def test_serving_matches_batch_on_long_and_stress_regions(engine):
     for tk, r, w in zip(tickets, regions, want):
         np.testing.assert_array_equal(e.drain(tk, r.num_pairs, timeout_ms=120000), w)
     e.close()
+
+
+def test_uneven_workload_full_size_properties():
+    """The uneven-length workload at its full size (20,000 regions, 10.9 M pairs):
+    every score finite and at most 0 (a probability), the chunked host pipeline
+    bitwise equal to one pass and to a repeated pass, and a random sample of
+    2,000 pairs within the tolerance of the oracle."""
+    from gpupairhmm_b200 import replicas
+    b = synth.config1(seed=1, regions=20000)
+    pinned = b.pin()
+    one = g.Engine(pipeline_chunks=1)
+    a = one.compute(pinned)
+    st = one.stats()
+    a2 = one.compute(pinned)
+    one.close()
+    chunked = g.Engine()  # 4 chunks at this size
+    c = chunked.compute(pinned)
+    chunked.close()
+    assert st.pairs == b.num_pairs == len(a) and st.rescued_ext == 0
+    assert np.isfinite(a).all() and (a <= 0.0).all()
+    np.testing.assert_array_equal(a, a2)
+    np.testing.assert_array_equal(a, c)
+    # a random sample of whole records through the oracle
+    rng = np.random.default_rng(5)
+    po = replicas.pair_offsets(b)
+    picks, n = [], 0
+    while n < 2000:
+        r = int(rng.integers(0, b.num_records))
+        picks.append(r)
+        n += int(po[r + 1] - po[r])
+    sub = synth.concat([b.select_records(r, r + 1) for r in picks])
+    got = np.concatenate([a[po[r]:po[r + 1]] for r in picks])
+    assert_log10_close(got, oracle.batch_log10(sub), what="uneven workload sample")
