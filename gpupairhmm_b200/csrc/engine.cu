@@ -955,7 +955,8 @@ pairhmm_status_t Engine::compute_host(const pairhmm_batch_t& b, float* scores) {
     if (b.num_records > 0 && b.reads_per_record && b.haps_per_record)
         for (int64_t g = 0; g < b.num_records; ++g)
             pairs += (int64_t)std::max(b.reads_per_record[g], 0) * std::max(b.haps_per_record[g], 0);
-    int nchunks = opts_.pipeline_chunks > 0 ? opts_.pipeline_chunks : (int)std::min<int64_t>(4, pairs / kChunkPairs);
+    int nchunks = opts_.pipeline_chunks > 0 ? opts_.pipeline_chunks
+                                             : (int)std::min<int64_t>(kMaxChunks, pairs / kChunkPairs);
     if (nchunks > b.num_records) nchunks = (int)b.num_records;
     if (nchunks < 2 || !b.read_lengths || !b.hap_lengths || !b.read_offsets || !b.hap_offsets) {
         pairhmm_status_t st = host_begin(b, scores, nullptr, nullptr);

@@ -104,9 +104,9 @@ typedef struct pairhmm_options {
     int32_t fp64_rescue;  /* 1 (default): recompute FP32 underflows in FP64 */
     int32_t use_graphs;   /* 1 (default): replay the per-batch launch sequence as a CUDA graph */
     int64_t device_budget_bytes; /* serving admission budget; 0 = 40 GiB */
-    int32_t pipeline_chunks; /* compute_host: 0 (default) = batches of 4M+ pairs run as up to
-                                4 chunks whose uploads overlap the previous chunk's kernels;
-                                1 = one pass; N = N chunks */
+    int32_t pipeline_chunks; /* compute_host: 0 (default) = batches of 2M+ pairs run as up to
+                                8 chunks of at least 1M pairs whose uploads overlap the previous
+                                chunk's kernels; 1 = one pass; N = N chunks */
     int32_t gcp;             /* 0 (default): eps = 0.1, beta = 0.9 for every pair, as the reference's
                                 GPU path (pairhmm_kernels.cuh:1195-1196; gcp qualities unused).
                                 1: eps = p(gcp), beta = 1 - eps per read, from the gcp quality
