@@ -333,7 +333,19 @@ def percentile(xs, q):
 def _serve_stream(eng, pool, times, picks, cells_of):
     """Submit pool regions at the given arrival times (busy wait), then collect.
     Latency of a region = (submission - arrival) + the engine's submit-to-done
-    time, so a submit loop that falls behind shows up in it."""
+    time, so a submit loop that falls behind shows up in it.  Python's cyclic
+    garbage collector is paused meanwhile (the loop allocates per region; a
+    collection would stall the submissions, not the service)."""
+    import gc
+    gc.collect()
+    gc.disable()
+    try:
+        return _serve_stream_timed(eng, pool, times, picks, cells_of)
+    finally:
+        gc.enable()
+
+
+def _serve_stream_timed(eng, pool, times, picks, cells_of):
     t0 = time.perf_counter()
     tickets = []
     for t_arr, i in zip(times, picks):
