@@ -8,7 +8,7 @@ import pytest
 ROOT = Path(__file__).resolve().parent.parent
 sys.path.insert(0, str(ROOT))
 
-# Parity tolerance on log10 likelihoods (the north-star bound is 1e-5 relative
+# Parity tolerance on log10 likelihoods (the accuracy bound is 1e-5 relative
 # on log10).  ATOL only matters for scores within 0.1 of zero, where a relative
 # bound alone would ask for more than FP32 arithmetic can carry.
 RTOL = 1e-5
