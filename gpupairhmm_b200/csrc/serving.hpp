@@ -11,7 +11,8 @@
 //
 // Regions with reads longer than the largest single tile (multi-tile work,
 // whose pairs each take a long serial wavefront) queue separately and run on
-// their own slot, so that a batch of short regions never waits behind them.
+// their own two slots, so that a batch of short regions never waits behind
+// them and a long region waits for at most one batch of long ones.
 #pragma once
 
 #include <chrono>
@@ -43,7 +44,7 @@ public:
     std::string last_error();
 
     static constexpr int kLightSlots = 2;          // regions of single-tile reads
-    static constexpr int kSlots = kLightSlots + 1;  // + one slot for multi-tile regions
+    static constexpr int kSlots = kLightSlots + 2;  // + two slots for multi-tile regions
 
 private:
     struct Region {

@@ -162,6 +162,8 @@ struct Fp64Wavefront {
                 if (p0 - 1 < L) qp = beta * (double)ph[(__ldg(rpack + p0 - 1) >> 16) & 0x7fu];
             }
             double aq[R], ee[R], rr[R], M[R], D[R];
+            // one division per position: 1/q of the previous position is carried
+            double iqp = 1.0 / qp;
 #pragma unroll
             for (int q = 0; q < Q; ++q) {
                 double lam[5][2];
@@ -181,10 +183,12 @@ struct Fp64Wavefront {
                     for (int h = 0; h < 5; ++h)
                         lam[h][s] = in ? ((x == 4u || h == 4 || x == (uint32_t)h) ? lm : lx) : 0.0;
                     const double qc = in ? beta * (double)d : beta;
-                    aq[r] = (double)(1.0f - (d + sg)) / qp;
-                    ee[r] = ((in ? epsd : 1.0) * qp) / qc;
-                    rr[r] = in ? (beta * (double)sg) / qc : 0.0;
+                    const double iqc = 1.0 / qc;
+                    aq[r] = (double)(1.0f - (d + sg)) * iqp;
+                    ee[r] = ((in ? epsd : 1.0) * qp) * iqc;
+                    rr[r] = in ? (beta * (double)sg) * iqc : 0.0;
                     qp = qc;
+                    iqp = iqc;
                     M[r] = 0.0;
                     D[r] = 0.0;
                 }

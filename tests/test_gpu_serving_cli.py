@@ -82,7 +82,7 @@ def test_serving_admission_under_a_small_budget():
     ref = g.Engine()
     want = [ref.compute(r) for r in regions]
     ref.close()
-    e = g.Engine(device_budget_bytes=3 * 400_000)
+    e = g.Engine(device_budget_bytes=4 * 400_000)  # four slots
     order = rng.permutation(len(regions))
     tickets = {int(i): e.submit(regions[i]) for i in order}
     for i, r in enumerate(regions):
