@@ -72,7 +72,7 @@ def parse_args():
     ap.add_argument("--serving-seconds", type=float, default=60.0,
                     help="length of the streaming-service run at --serving-rate (0 = skip)")
     ap.add_argument("--serving-rate", type=float, default=2000.0, help="region arrivals per second")
-    ap.add_argument("--sweep-rates", default="8000,20000,40000,80000",
+    ap.add_argument("--sweep-rates", default="8000,20000,40000,60000",
                     help="further arrival rates of the serving sweep (comma separated, '' = none); "
                          "stops at the first rate whose p99 exceeds 1 s")
     ap.add_argument("--sweep-seconds", type=float, default=10.0)
@@ -330,42 +330,62 @@ def percentile(xs, q):
     return float(np.percentile(np.asarray(xs, dtype=np.float64), q)) if len(xs) else None
 
 
-def _serve_stream(eng, pool, times, picks, cells_of):
-    """Submit pool regions at the given arrival times (busy wait), then collect.
-    Latency of a region = (submission - arrival) + the engine's submit-to-done
-    time, so a submit loop that falls behind shows up in it.  Python's cyclic
-    garbage collector is paused meanwhile (the loop allocates per region; a
+def _serve_stream(eng, pool, times, picks, cells_of, heavy=None):
+    """Submit pool regions at the given arrival times, then collect.  Every
+    pass of the loop submits all regions that have arrived by then in one
+    ``submit_many`` call (busy wait while none is due).  Latency of a region =
+    (call start - arrival) + the engine's submit-to-done time (which counts
+    from the start of the call), so a submit loop that falls behind shows up
+    in it.  Python's cyclic garbage collector is paused meanwhile (a
     collection would stall the submissions, not the service)."""
     import gc
     gc.collect()
     gc.disable()
     try:
-        return _serve_stream_timed(eng, pool, times, picks, cells_of)
+        return _serve_stream_timed(eng, pool, times, picks, cells_of, heavy)
     finally:
         gc.enable()
 
 
-def _serve_stream_timed(eng, pool, times, picks, cells_of):
+def _serve_stream_timed(eng, pool, times, picks, cells_of, heavy):
+    times = np.asarray(times, dtype=np.float64)
+    n = len(times)
     t0 = time.perf_counter()
-    tickets = []
-    for t_arr, i in zip(times, picks):
-        while time.perf_counter() - t0 < t_arr:
-            pass
-        t_sub = time.perf_counter() - t0
-        tickets.append((eng.submit(pool[i]), t_sub, t_sub - t_arr, pool[i].num_pairs))
+    tickets, sub, late = [], np.zeros(n), np.zeros(n)
+    k = 0
+    calls = 0
+    while k < n:
+        now = time.perf_counter() - t0
+        if now < times[k]:
+            continue
+        j = int(np.searchsorted(times, now, side="right"))
+        tickets += eng.submit_many(pool, picks[k:j])
+        sub[k:j] = now
+        late[k:j] = now - times[k:j]
+        calls += 1
+        k = j
     lat, done = [], []
-    for tk, t_sub, late, n in tickets:
+    for i, tk in enumerate(tickets):
         while not eng.poll(tk):
             time.sleep(0.0002)
         ms = eng.latency_ms(tk)
-        eng.drain(tk, n)
-        lat.append(late * 1e3 + ms)
-        done.append(t_sub + ms / 1e3)
+        eng.drain(tk, pool.num_pairs[picks[i]])
+        lat.append(late[i] * 1e3 + ms)
+        done.append(sub[i] + ms / 1e3)
     span = max(done) if done else 1e-9
     cells = sum(cells_of[i] for i in picks)
-    return {"regions": len(times), "p50_ms": round(percentile(lat, 50), 3), "p99_ms": round(percentile(lat, 99), 3),
-            "max_ms": round(max(lat), 3), "gcups": round(cells / span / 1e9, 3), "span_s": round(span, 3),
-            "offered_gcups": round(cells / max(float(times[-1]), 1e-9) / 1e9, 3) if len(times) else 0.0}
+    out = {"regions": n, "submit_calls": calls, "p50_ms": round(percentile(lat, 50), 3),
+           "p99_ms": round(percentile(lat, 99), 3), "max_ms": round(max(lat), 3) if lat else 0.0,
+           "gcups": round(cells / span / 1e9, 3), "span_s": round(span, 3),
+           "offered_gcups": round(cells / max(float(times[-1]), 1e-9) / 1e9, 3) if n else 0.0}
+    if heavy is not None and n:
+        kind = np.asarray([heavy[i] for i in picks])
+        lat = np.asarray(lat)
+        for name, sel in (("single_tile", ~kind), ("multi_tile", kind)):
+            if sel.any():
+                out[name] = {"regions": int(sel.sum()), "p50_ms": round(percentile(lat[sel], 50), 3),
+                             "p99_ms": round(percentile(lat[sel], 99), 3)}
+    return out
 
 
 def run_serving(args, local_rank):
@@ -379,22 +399,26 @@ def run_serving(args, local_rank):
     per region in arrival order (latency from arrival)."""
     import gpupairhmm_b200 as g
     from gpupairhmm_b200 import synth
-    pool = synth.region_pool(seed=4, regions=24000, long_frac=0.05)
-    cells_of = [r.cells() for r in pool]
+    pool = g.RegionSet(synth.region_pool(seed=4, regions=24000, long_frac=0.05))
+    cells_of = [r.cells() for r in pool.regions]
     times, picks = synth.poisson_arrivals(5, args.serving_rate, args.serving_seconds, len(pool))
     out = {"rate_per_s": args.serving_rate, "seconds": args.serving_seconds, "long_region_fraction": 0.05,
            "pool": "24,000 regions drawn ahead of time (seed 4), picked uniformly per arrival",
            "latency": "arrival to scores on the host (submission delay + submit-to-done)"}
 
     eng = g.Engine(device=local_rank)
-    warm = [eng.submit(r) for r in pool[:300]]  # warm the queue's engines (a burst of both kinds)
-    for tk, r in zip(warm, pool[:300]):
-        eng.drain(tk, r.num_pairs)
-    out["continuous_batching"] = _serve_stream(eng, pool, times, picks, cells_of)
+    # regions with a read beyond the longest single tile run on the multi-tile slots
+    single_max = max(m for m, _, _, kind in eng.tile_table() if kind != 1)
+    heavy = [int(np.max(r.read_lengths)) > single_max for r in pool.regions]
+    warm = eng.submit_many(pool, range(300))  # warm the queue's engines (a burst of both kinds)
+    for i, tk in enumerate(warm):
+        eng.drain(tk, pool.num_pairs[i])
+    out["continuous_batching"] = _serve_stream(eng, pool, times, picks, cells_of, heavy)
     sweep = []
     for k, rate in enumerate(float(x) for x in args.sweep_rates.split(",") if x.strip()):
         tt, pp = synth.poisson_arrivals(6 + k, rate, args.sweep_seconds, len(pool))
-        point = dict(rate_per_s=rate, seconds=args.sweep_seconds, **_serve_stream(eng, pool, tt, pp, cells_of))
+        point = dict(rate_per_s=rate, seconds=args.sweep_seconds,
+                     **_serve_stream(eng, pool, tt, pp, cells_of, heavy))
         sweep.append(point)
         if point["p99_ms"] > 1000.0:
             break
@@ -404,7 +428,7 @@ def run_serving(args, local_rank):
 
     # one region per blocking call, plain FP32 form, first 10 s of the stream
     pe = g.Engine(device=local_rank, mode=g.MODE_PLAIN)
-    for r in pool[:200]:
+    for r in pool.regions[:200]:
         pe.compute(r)
     n10 = int(np.searchsorted(times, min(10.0, args.serving_seconds), side="right"))
     lat = []

@@ -116,6 +116,7 @@ _SIGNATURES = {
     "pairhmm_compute_device": (ctypes.c_int, [_P, _P, ctypes.c_int32, ctypes.c_int32, _P, _P]),
     "pairhmm_get_stats": (ctypes.c_int, [_P, _P]),
     "pairhmm_submit": (ctypes.c_int, [_P, _P, _P]),
+    "pairhmm_submit_many": (ctypes.c_int, [_P, _P, ctypes.c_int64, _P]),
     "pairhmm_poll": (ctypes.c_int, [_P, ctypes.c_uint64, _P]),
     "pairhmm_drain": (ctypes.c_int, [_P, ctypes.c_uint64, _P, ctypes.c_int64, ctypes.c_int32]),
     "pairhmm_region_latency_ms": (ctypes.c_int, [_P, ctypes.c_uint64, _P]),
@@ -176,6 +177,23 @@ def _ptr(a) -> int | None:
         return a.ctypes.data
     # torch tensors (host or device)
     return a.data_ptr()
+
+
+class RegionSet:
+    """Regions prepared once for repeated serving submissions: arrays made
+    contiguous and their C descriptors built ahead (``Engine.submit_many``
+    then only copies descriptors)."""
+
+    def __init__(self, regions):
+        self.regions = [r.contiguous() for r in regions]
+        self.structs = [r.as_struct() for r in self.regions]
+        self.num_pairs = [r.num_pairs for r in self.regions]
+
+    def __len__(self) -> int:
+        return len(self.regions)
+
+    def __getitem__(self, i: int) -> "Batch":
+        return self.regions[i]
 
 
 @dataclass
@@ -349,6 +367,25 @@ class Engine:
         s = r.as_struct()
         _check(lib().pairhmm_submit(self._h, ctypes.byref(s), ctypes.byref(t)), self._h)
         return int(t.value)
+
+    def submit_many(self, regions, picks=None) -> list[int]:
+        """Submit several regions in one call (one lock, one wake-up of the
+        serving slots); returns their tickets in order.  ``regions`` is a list
+        of batches, or a ``RegionSet`` with ``picks`` the indices to submit
+        (a region may be picked more than once).  On an error none is queued."""
+        if isinstance(regions, RegionSet):
+            idx = range(len(regions)) if picks is None else picks
+            structs = regions.structs
+            arr = (_Batch * len(idx))(*[structs[i] for i in idx])
+        else:
+            keep = [r.contiguous() for r in regions]
+            arr = (_Batch * len(keep))(*[r.as_struct() for r in keep])
+        n = len(arr)
+        if n == 0:
+            return []
+        t = (ctypes.c_uint64 * n)()
+        _check(lib().pairhmm_submit_many(self._h, arr, n, t), self._h)
+        return list(t)
 
     def poll(self, ticket: int) -> bool:
         d = ctypes.c_int32()

@@ -148,6 +148,15 @@ pairhmm_status_t pairhmm_submit(pairhmm_engine_t* h, const pairhmm_batch_t* regi
     });
 }
 
+pairhmm_status_t pairhmm_submit_many(pairhmm_engine_t* h, const pairhmm_batch_t* regions, int64_t num_regions,
+                                     uint64_t* tickets) {
+    if (!h || num_regions < 0 || (num_regions > 0 && (!regions || !tickets))) return PAIRHMM_ERR_INVALID_ARGUMENT;
+    return guarded(h, [&] {
+        phmm::ServingQueue* q = serving_of(h, true);
+        return serving_result(h, q, q->submit_many(regions, num_regions, tickets));
+    });
+}
+
 pairhmm_status_t pairhmm_poll(pairhmm_engine_t* h, uint64_t ticket, int32_t* done) {
     if (!h || !done) return PAIRHMM_ERR_INVALID_ARGUMENT;
     return guarded(h, [&] {

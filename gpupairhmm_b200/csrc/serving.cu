@@ -1,5 +1,6 @@
 #include <algorithm>
 #include <cstring>
+#include <string>
 
 #include "serving.hpp"
 
@@ -59,26 +60,14 @@ int64_t ServingQueue::estimate_device_bytes(const Region& r) {
            r.pairs * (16 + 16 + 4) + reads * 32 + haps * 24 + 4096;
 }
 
-pairhmm_status_t ServingQueue::submit(const pairhmm_batch_t& b, uint64_t* ticket) {
-    BatchIndex x;
-    std::string err;
-    pairhmm_status_t st = Engine::build_index(b, parent_.tile_table(), x, err);
-    if (st != PAIRHMM_OK) {
-        std::lock_guard<std::mutex> lk(mu_);
-        return set_error(st, err.c_str());
-    }
+pairhmm_status_t ServingQueue::prepare(const pairhmm_batch_t& b, std::shared_ptr<Region>& out,
+                                       std::string& err) const {
+    // the checks of a batch call (counts, null arrays, lengths, offsets, gcp),
+    // without building its work list: the slot's merged batch builds that
+    InputRanges x;
     const bool gcp = parent_.gcp();
-    const char* bad = nullptr;
-    if (x.num_reads > 0 && (!b.read_bases || !b.base_quals || !b.ins_quals || !b.del_quals || !b.read_offsets))
-        bad = "null read arrays";
-    else if (x.num_haps > 0 && (!b.hap_bases || !b.hap_offsets))
-        bad = "null haplotype arrays";
-    else if (gcp && x.num_reads > 0 && !b.gcp_quals)
-        bad = "gcp mode needs the gcp quality array";
-    if (bad) {
-        std::lock_guard<std::mutex> lk(mu_);
-        return set_error(PAIRHMM_ERR_INVALID_ARGUMENT, bad);
-    }
+    const pairhmm_status_t st = Engine::scan_inputs(b, x, err, gcp);
+    if (st != PAIRHMM_OK) return st;
     auto r = std::make_shared<Region>();
     r->rpr.assign(b.reads_per_record, b.reads_per_record + b.num_records);
     r->hpr.assign(b.haps_per_record, b.haps_per_record + b.num_records);
@@ -88,7 +77,12 @@ pairhmm_status_t ServingQueue::submit(const pairhmm_batch_t& b, uint64_t* ticket
     r->read_off.resize(x.num_reads);
     r->hap_off.resize(x.num_haps);
     int64_t total = 0;
-    for (int64_t i = 0; i < x.num_reads; ++i) { r->read_off[i] = total; total += b.read_lengths[i]; }
+    int32_t max_read_len = 0;
+    for (int64_t i = 0; i < x.num_reads; ++i) {
+        r->read_off[i] = total;
+        total += b.read_lengths[i];
+        max_read_len = std::max(max_read_len, b.read_lengths[i]);
+    }
     r->read_bases.resize(total);
     r->bq.resize(total);
     r->iq.resize(total);
@@ -108,13 +102,18 @@ pairhmm_status_t ServingQueue::submit(const pairhmm_batch_t& b, uint64_t* ticket
     for (int64_t h = 0; h < x.num_haps; ++h)
         std::memcpy(&r->hap_bases[r->hap_off[h]], b.hap_bases + b.hap_offsets[h], b.hap_lengths[h]);
     r->pairs = x.num_pairs;
-    r->heavy = x.max_read_len > single_tile_max_;
+    r->heavy = max_read_len > single_tile_max_;
     r->device_bytes = estimate_device_bytes(*r);
     if (r->device_bytes > budget_per_slot_) {
-        std::lock_guard<std::mutex> lk(mu_);
-        return set_error(PAIRHMM_ERR_BUDGET, "region needs more device memory than one batch slot's budget");
+        err = "region needs more device memory than one batch slot's budget";
+        return PAIRHMM_ERR_BUDGET;
     }
-    r->t_submit = std::chrono::steady_clock::now();
+    out = std::move(r);
+    return PAIRHMM_OK;
+}
+
+pairhmm_status_t ServingQueue::enqueue(const std::vector<std::shared_ptr<Region>>& rs,
+                                       std::chrono::steady_clock::time_point t_submit, uint64_t* tickets) {
     {
         std::lock_guard<std::mutex> lk(mu_);
         if (engines_.empty()) {
@@ -125,7 +124,7 @@ pairhmm_status_t ServingQueue::submit(const pairhmm_batch_t& b, uint64_t* ticket
                 o.fp64_rescue = 1;
                 o.use_graphs = 1;
                 o.pipeline_chunks = 1;  // merged batches stay small: one pass
-                o.gcp = gcp ? 1 : 0;
+                o.gcp = parent_.gcp() ? 1 : 0;
                 auto e = std::make_unique<Engine>(o);
                 pairhmm_status_t is = e->init();
                 if (is == PAIRHMM_OK) is = e->set_tile_table(parent_.tile_table());
@@ -138,13 +137,41 @@ pairhmm_status_t ServingQueue::submit(const pairhmm_batch_t& b, uint64_t* ticket
             }
             for (int s = 0; s < kSlots; ++s) threads_.emplace_back(&ServingQueue::worker, this, s);
         }
-        r->ticket = next_ticket_++;
-        tickets_[r->ticket] = r;
-        (r->heavy ? heavy_ : light_).push_back(r);
-        *ticket = r->ticket;
+        for (size_t i = 0; i < rs.size(); ++i) {
+            const std::shared_ptr<Region>& r = rs[i];
+            r->t_submit = t_submit;
+            r->ticket = next_ticket_++;
+            tickets_[r->ticket] = r;
+            (r->heavy ? heavy_ : light_).push_back(r);
+            tickets[i] = r->ticket;
+        }
     }
     cv_work_.notify_all();
     return PAIRHMM_OK;
+}
+
+pairhmm_status_t ServingQueue::submit(const pairhmm_batch_t& b, uint64_t* ticket) {
+    return submit_many(&b, 1, ticket);
+}
+
+pairhmm_status_t ServingQueue::submit_many(const pairhmm_batch_t* regions, int64_t n, uint64_t* tickets) {
+    if (n < 0 || (n > 0 && (!regions || !tickets))) {
+        std::lock_guard<std::mutex> lk(mu_);
+        return set_error(PAIRHMM_ERR_INVALID_ARGUMENT, "bad region list");
+    }
+    const auto t_submit = std::chrono::steady_clock::now();  // latency counts the copies below
+    std::vector<std::shared_ptr<Region>> rs((size_t)n);
+    for (int64_t i = 0; i < n; ++i) {
+        std::string err;
+        const pairhmm_status_t st = prepare(regions[i], rs[(size_t)i], err);
+        if (st != PAIRHMM_OK) {
+            if (n > 1) err = "region " + std::to_string(i) + ": " + err;
+            std::lock_guard<std::mutex> lk(mu_);
+            return set_error(st, err.c_str());
+        }
+    }
+    if (n == 0) return PAIRHMM_OK;
+    return enqueue(rs, t_submit, tickets);
 }
 
 void ServingQueue::worker(int slot) {
@@ -200,6 +227,10 @@ void ServingQueue::worker(int slot) {
             dq.insert(dq.end(), r->dq.begin(), r->dq.end());
             gq.insert(gq.end(), r->gq.begin(), r->gq.end());
             hb.insert(hb.end(), r->hap_bases.begin(), r->hap_bases.end());
+            // the merged copy is all the batch needs: give the region's input copy back now
+            // rather than when it is drained (a client that drains late would otherwise hold
+            // every input it submitted meanwhile)
+            r->release_inputs();
         }
         pairhmm_batch_t b{};
         b.num_records = (int64_t)rpr.size();

@@ -2,7 +2,7 @@
 // only processes whole files: gpuworker.cuh:435-471).
 //
 // submit() copies a region (one or more records) into host memory and queues
-// it.  kSlots worker threads each own an Engine (own stream and device
+// it (submit_many() takes many regions per call).  kSlots worker threads each own an Engine (own stream and device
 // buffers); a worker that becomes free takes every queued region that fits its
 // share of the device budget, merges them into one batch, runs it, and
 // completes the tickets.  While one slot's batch runs on the GPU the next slot
@@ -36,6 +36,9 @@ public:
     ~ServingQueue();
 
     pairhmm_status_t submit(const pairhmm_batch_t& region, uint64_t* ticket);
+    // n regions under one lock and one wake-up; all are checked and copied
+    // before any is queued, so an error queues none of them
+    pairhmm_status_t submit_many(const pairhmm_batch_t* regions, int64_t n, uint64_t* tickets);
     pairhmm_status_t poll(uint64_t ticket, int32_t* done);
     pairhmm_status_t drain(uint64_t ticket, float* scores, int64_t num_scores, int32_t timeout_ms);
     pairhmm_status_t latency(uint64_t ticket, double* ms);
@@ -60,9 +63,21 @@ private:
         bool done = false;
         pairhmm_status_t status = PAIRHMM_OK;
         std::string error;
+        // after the merge only the counts, pairs and results are used
+        void release_inputs() {
+            for (auto* v : {&rpr, &hpr, &read_len, &hap_len}) std::vector<int32_t>().swap(*v);
+            std::vector<int64_t>().swap(read_off);
+            std::vector<int64_t>().swap(hap_off);
+            for (auto* v : {&read_bases, &bq, &iq, &dq, &gq, &hap_bases}) std::vector<uint8_t>().swap(*v);
+        }
     };
 
     void worker(int slot);
+    // checks a region and copies it into host memory owned by the queue (no lock held)
+    pairhmm_status_t prepare(const pairhmm_batch_t& b, std::shared_ptr<Region>& out, std::string& err) const;
+    // gives the regions tickets and queues them (starts the slots on first use)
+    pairhmm_status_t enqueue(const std::vector<std::shared_ptr<Region>>& rs,
+                             std::chrono::steady_clock::time_point t_submit, uint64_t* tickets);
     static int64_t estimate_device_bytes(const Region& r);
     pairhmm_status_t set_error(pairhmm_status_t s, const char* msg);  // caller holds mu_
 

@@ -189,6 +189,10 @@ struct Fp32Wavefront {
                 }
             }
             float qp = q_prev;
+            // Single-tile kernels carry 1/alpha forward (two divisions per position instead of
+            // four); the multi-tile kernel keeps the divisions, its 255-register budget spills
+            // with the extra live value.
+            float ia = MT ? 1.0f : 1.0f / a_cur[0];
 #pragma unroll
             for (int g = 0; g < NGRP; ++g) {
                 uint32_t ws[4];
@@ -210,11 +214,21 @@ struct Fp32Wavefront {
                     for (int h = 0; h < 5; ++h)
                         lam[h][s] = in ? an * ((x == 4u || h == 4 || x == (uint32_t)h) ? lm : lx) : 0.0f;
                     if (in && !(fabsf(a_cur[r]) >= kMinAlpha)) degenerate = true;
-                    const float qc = in ? (beta * d) / a_cur[r] : beta;  // I scale of c
                     dpv[r] = qp;
-                    ee[r] = ((in ? eps : 1.0f) * qp) / qc;
-                    rr[r] = in ? ((beta * sg) / an) / qc : 0.0f;
-                    qp = qc;
+                    if constexpr (MT) {
+                        const float qc = in ? (beta * d) / a_cur[r] : beta;  // I scale of c
+                        ee[r] = ((in ? eps : 1.0f) * qp) / qc;
+                        rr[r] = in ? ((beta * sg) / an) / qc : 0.0f;
+                        qp = qc;
+                    } else {
+                        const float ian = 1.0f / an;
+                        const float qc = in ? (beta * d) * ia : beta;  // I scale of c
+                        const float iqc = 1.0f / qc;
+                        ee[r] = ((in ? eps : 1.0f) * qp) * iqc;
+                        rr[r] = in ? ((beta * sg) * ian) * iqc : 0.0f;
+                        qp = qc;
+                        ia = ian;
+                    }
                     N[r] = 0.0f;
                     D[r] = 0.0f;
                 }

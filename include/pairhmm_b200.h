@@ -20,17 +20,18 @@
  *   GpuPairHMMWorker::computeNumberOfDPCells
  *     (gpuworker.cuh:495-520) and the GCUPS print
  *     (gpuworker.cuh:426-427)                              pairhmm_get_stats
- *   (no counterpart: the reference has no serving mode)    pairhmm_submit / _poll / _drain
+ *   (no counterpart: the reference has no serving mode)    pairhmm_submit / _submit_many /
+ *                                                          _poll / _drain
  *
  * Scores: one float log10 likelihood per (read, haplotype) pair, written at
  * slot  sum_{previous records} R*H + r*H + h  (gpuworker.cuh:1002-1021,
  * pairhmm_kernels.cuh:1154).
  *
  * Threading: an engine is used by one host thread at a time (as the
- * reference's worker is), except for the serving calls (submit, poll, drain,
- * region_latency_ms, serving_stats), which may overlap from several threads
- * (a producer submitting while a consumer drains).  Different engines are
- * independent.
+ * reference's worker is), except for the serving calls (submit, submit_many,
+ * poll, drain, region_latency_ms, serving_stats), which may overlap from
+ * several threads (a producer submitting while a consumer drains).  Different
+ * engines are independent.
  */
 #ifndef PAIRHMM_B200_H
 #define PAIRHMM_B200_H
@@ -157,13 +158,19 @@ pairhmm_status_t pairhmm_compute_device(pairhmm_engine_t* engine, const pairhmm_
 
 pairhmm_status_t pairhmm_get_stats(pairhmm_engine_t* engine, pairhmm_stats_t* stats);
 
-/* Serving (continuous batching).  submit copies the region to pinned staging
- * and returns a ticket; regions submitted while others run are admitted into
- * the device work queue as memory under the budget frees up.  poll reports
- * completion without blocking; drain blocks (bounded by timeout_ms, <0 =
- * forever) and copies the scores out, releasing the ticket. */
+/* Serving (continuous batching).  submit copies the region into host memory
+ * owned by the queue and returns a ticket; regions submitted while others run
+ * are admitted into the device work queue as memory under the budget frees
+ * up.  poll reports completion without blocking; drain blocks (bounded by
+ * timeout_ms, <0 = forever) and copies the scores out, releasing the ticket. */
 pairhmm_status_t pairhmm_submit(pairhmm_engine_t* engine, const pairhmm_batch_t* region,
                                 uint64_t* ticket);
+/* num_regions regions in one call (one lock, one wake-up of the slots);
+ * tickets[i] is region i's.  Every region is checked and copied before any is
+ * queued: on an error none is queued and the error text names the region.
+ * A region's latency counts from the start of the call. */
+pairhmm_status_t pairhmm_submit_many(pairhmm_engine_t* engine, const pairhmm_batch_t* regions,
+                                     int64_t num_regions, uint64_t* tickets);
 pairhmm_status_t pairhmm_poll(pairhmm_engine_t* engine, uint64_t ticket, int32_t* done);
 pairhmm_status_t pairhmm_drain(pairhmm_engine_t* engine, uint64_t ticket, float* scores,
                                int64_t num_scores, int32_t timeout_ms);

@@ -121,6 +121,46 @@ def test_serving_concurrent_drains_of_one_ticket():
     e.close()
 
 
+def test_submit_many_matches_the_batch_call():
+    """Regions submitted many per call -- a list, and a prepared region set with
+    a region picked more than once -- give the batch call's scores bitwise."""
+    regions = [synth.config1(seed=900 + i, regions=1) for i in range(20)] + [synth.config3(seed=901, regions=1)]
+    ref = g.Engine()
+    alone = [ref.compute(r) for r in regions]
+    ref.close()
+    e = g.Engine()
+    tickets = e.submit_many(regions)
+    assert len(set(tickets)) == len(regions)
+    for t, r, want in zip(tickets, regions, alone):
+        np.testing.assert_array_equal(e.drain(t, r.num_pairs, timeout_ms=120000), want)
+    rs = g.RegionSet(regions)
+    picks = np.array([3, 3, 20, 0, 7, 3])
+    tickets = e.submit_many(rs, picks)
+    for t, i in zip(tickets, picks):
+        np.testing.assert_array_equal(e.drain(t, rs.num_pairs[i], timeout_ms=120000), alone[i])
+    assert e.submit_many([]) == []
+    e.close()
+
+
+def test_submit_many_queues_nothing_when_a_region_is_bad():
+    """One malformed region fails the whole call, names the region, and leaves
+    the queue as it was."""
+    good = [synth.config0(seed=10 + i, records=1) for i in range(4)]
+    bad = synth.config0(seed=20, records=1)
+    bad.read_lengths = np.array(bad.read_lengths, dtype=np.int32)
+    bad.read_lengths[1] = 0
+    e = g.Engine()
+    with pytest.raises(g.PairHMMError) as err:
+        e.submit_many(good[:2] + [bad] + good[2:])
+    assert err.value.status == 1
+    assert "region 2" in str(err.value)
+    tickets = e.submit_many(good)
+    for t, r in zip(tickets, good):
+        assert_log10_close(e.drain(t, r.num_pairs, timeout_ms=60000), oracle.batch_log10(r), what="served")
+    assert e.serving_stats()["regions"] == len(good)
+    e.close()
+
+
 def test_cli_end_to_end(tmp_path):
     b = synth.config0(seed=7, records=6)
     text = synth.to_text(b) + synth.to_text(synth.config3(seed=8, regions=1))
