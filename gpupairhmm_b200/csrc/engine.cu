@@ -153,6 +153,16 @@ pairhmm_status_t Engine::cuda_fail(cudaError_t e, const char* what) {
         if (e_ != cudaSuccess) return cuda_fail(e_, #call); \
     } while (0)
 
+pairhmm_status_t Engine::reserve_pool(size_t bytes) {
+    if (!pool_ || bytes == 0) return PAIRHMM_OK;
+    PHMM_CUDA(cudaSetDevice(opts_.device));
+    void* p = nullptr;
+    PHMM_CUDA(cudaMallocFromPoolAsync(&p, bytes, pool_, stream_));
+    PHMM_CUDA(cudaFreeAsync(p, stream_));
+    PHMM_CUDA(cudaStreamSynchronize(stream_));
+    return PAIRHMM_OK;
+}
+
 pairhmm_status_t Engine::init() {
     int ndev = 0;
     cudaError_t e = cudaGetDeviceCount(&ndev);

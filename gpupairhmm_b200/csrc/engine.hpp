@@ -71,6 +71,9 @@ public:
     Engine& operator=(const Engine&) = delete;
 
     pairhmm_status_t init();
+    // keeps `bytes` of device memory in the engine's pool (allocated once and freed), so
+    // that buffer growth up to that size maps no new memory while other work runs
+    pairhmm_status_t reserve_pool(size_t bytes);
     pairhmm_status_t compute_host(const pairhmm_batch_t& b, float* scores);
     pairhmm_status_t compute_device(const pairhmm_batch_t& b, int32_t max_read_len, int32_t max_hap_len,
                                     float* scores, cudaStream_t stream);

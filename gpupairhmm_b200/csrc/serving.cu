@@ -9,6 +9,7 @@ namespace phmm {
 namespace {
 constexpr int64_t kDefaultBudget = int64_t(40) << 30;  // 40 GiB
 constexpr int64_t kMaxBatchPairs = int64_t(4) << 20;   // cap on pairs merged into one batch
+constexpr int64_t kReservePerSlot = int64_t(3) << 30;  // device memory a slot keeps from its start
 }  // namespace
 
 ServingQueue::ServingQueue(Engine& parent) : parent_(parent) {
@@ -128,6 +129,10 @@ pairhmm_status_t ServingQueue::enqueue(const std::vector<std::shared_ptr<Region>
                 auto e = std::make_unique<Engine>(o);
                 pairhmm_status_t is = e->init();
                 if (is == PAIRHMM_OK) is = e->set_tile_table(parent_.tile_table());
+                // device memory for the slot's batches up front (its budget, at most
+                // kReservePerSlot): a batch larger than any before then grows its buffers
+                // inside the pool instead of mapping memory while the other slots run
+                if (is == PAIRHMM_OK) is = e->reserve_pool((size_t)std::min(budget_per_slot_, kReservePerSlot));
                 if (is != PAIRHMM_OK) {
                     error_ = e->last_error();
                     engines_.clear();
