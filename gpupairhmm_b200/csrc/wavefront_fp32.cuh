@@ -59,6 +59,9 @@
 // i writes (X^, I^, N) of its last position for every haplotype row into a
 // per-group scratch border, which lane 0 of tile i+1 reads as its left
 // boundary (pairhmm_kernels.cuh:2167-3272 does the same with 512-row tiles).
+// The group's lanes fetch those rows G at a time from L2 one block ahead and
+// put them in a per-warp shared ring, from which each step takes its row with
+// one broadcast load (three shuffles per step before).
 //
 // Early hand-off of long pairs that will underflow: every path to the result
 // crosses the border column once, and transitions and emissions never exceed
@@ -85,7 +88,9 @@ struct Fp32Wavefront {
     static constexpr bool kTail = R % 4 == 2;       // then one float2 group after them
     static constexpr int NGRP = Q + (kTail ? 1 : 0);  // position groups: 4 each, the tail 2
     static constexpr int kTail2 = 5 * Q * 32;       // float4 index where the float2 tail table starts
-    static constexpr int kTableFloat4 = 5 * Q * 32 + (kTail ? 5 * 32 / 2 : 0);  // per warp
+    static constexpr int kLamFloat4 = 5 * Q * 32 + (kTail ? 5 * 32 / 2 : 0);
+    // per warp: the lam' table, then (MT) a 32-entry ring of border rows
+    static constexpr int kTableFloat4 = kLamFloat4 + (MT ? 32 : 0);
 
     __host__ __device__ static constexpr int group_size(int g) { return g < Q ? 4 : 2; }
 
@@ -274,13 +279,12 @@ struct Fp32Wavefront {
             float4* ein = nullptr;
             float4* eout = nullptr;
             const int64_t nrow = rows - G;  // rows a buffer holds after the padding
-            float4 bcur = make_float4(0.f, 0.f, 0.f, 0.f), bnext = bcur;
+            float4 bcur = make_float4(0.f, 0.f, 0.f, 0.f);  // lane t: row t of the next block of G
             if (MT) {
                 float4* gbase = scratch + (int64_t)grp * 2 * rows;
                 if (tile > 0) {
                     ein = gbase + ((tile - 1) & 1) * rows + G;
                     if (t < nrow) bcur = __ldcg(ein + t);
-                    if (G + t < nrow) bnext = __ldcg(ein + G + t);
                 }
                 eout = gbase + (tile & 1) * rows + G;
             }
@@ -293,8 +297,17 @@ struct Fp32Wavefront {
             const int wlast = ((Hc + 15) & ~15) / 4 - 1;
             uint32_t wcur = __ldg(hw);
             uint32_t wnext = __ldg(hw + 1);
+            float4* ring = wtab + kLamFloat4;  // MT: rows of the group's current block of G steps
             for (int k0 = 0; k0 < K; k0 += 4) {
                 const uint32_t wpref = __ldg(hw + min_i((k0 >> 2) + 2, wlast));
+                if (MT && tile > 0 && (k0 & (G - 1)) == 0) {
+                    // lane t of the group holds row k0 + t: into the ring, then prefetch
+                    __syncwarp();
+                    ring[lane] = bcur;
+                    __syncwarp();
+                    const int64_t idx = (int64_t)k0 + G + t;
+                    bcur = idx < nrow ? __ldcg(ein + idx) : make_float4(0.f, 0.f, 0.f, 0.f);
+                }
                 float acc = 0.f;
 #pragma unroll
                 for (int s = 0; s < 4; ++s) {
@@ -347,18 +360,10 @@ struct Fp32Wavefront {
                     Iul = __shfl_up_sync(kFullMask, Idiag, 1, G);
                     Xul = __shfl_up_sync(kFullMask, Xdiag, 1, G);
                     if (MT && tile > 0) {
-                        const int src = k & (G - 1);
-                        const float bx = __shfl_sync(kFullMask, bcur.x, src, G);
-                        const float by = __shfl_sync(kFullMask, bcur.y, src, G);
-                        const float bz = __shfl_sync(kFullMask, bcur.z, src, G);
                         // the border is indexed by row: it feeds the diagonal of the next
                         // step directly (lanes t > 0 get theirs through the Ml -> Mul rotation)
-                        if (t == 0) { Xul = bx; Iul = by; Mul = bz; }
-                        if (src == G - 1) {
-                            bcur = bnext;
-                            const int64_t idx = (int64_t)k + 1 + G + t;
-                            bnext = idx < nrow ? __ldcg(ein + idx) : make_float4(0.f, 0.f, 0.f, 0.f);
-                        }
+                        const float4 brow = ring[grp * G + (k & (G - 1))];  // broadcast within the group
+                        if (t == 0) { Xul = brow.x; Iul = brow.y; Mul = brow.z; }
                     } else if (t == 0) {
                         Ml = 0.f;
                         Iul = 0.f;

@@ -269,6 +269,11 @@ struct Fp64Wavefront {
                             e -= over;
                         }
                     }
+                    // border row for the next step's diagonal, loaded before this step's cells
+                    // so the shared-memory latency overlaps them (every lane takes part in the
+                    // broadcast load, lane 0 keeps it)
+                    Border bk{};
+                    if (MT && tile > 0) bk = ring[k & (kRing - 1)];
                     double Mdiag = Mul, Idiag = Iul, Xdiag = Xul;
                     if constexpr (EXT) {
                         const double fM = pow2i(e - eMul);
@@ -316,13 +321,11 @@ struct Fp64Wavefront {
                         eIul = es;
                     }
                     if (MT && tile > 0) {
-                        // the border is indexed by row: it feeds the next step's diagonal;
-                        // every lane takes part in the (broadcast) load, lane 0 keeps it
-                        const Border b = ring[k & (kRing - 1)];
+                        // the border is indexed by row: it feeds the next step's diagonal
                         if (t == 0) {
                             const bool in = k < Hc;
-                            Mul = in ? b.m : 0.0; Xul = in ? b.x : 0.0; Iul = in ? b.i : 0.0;
-                            eMul = in ? border_e(b) : 0; eIul = in ? border_ei(b) : 0;
+                            Mul = in ? bk.m : 0.0; Xul = in ? bk.x : 0.0; Iul = in ? bk.i : 0.0;
+                            eMul = in ? border_e(bk) : 0; eIul = in ? border_ei(bk) : 0;
                         }
                     } else if (t == 0) {
                         Ml = 0.0; Iul = 0.0; Xul = Dbound; eMl = 0; eIul = 0;
