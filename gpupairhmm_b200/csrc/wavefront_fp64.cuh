@@ -10,8 +10,10 @@
 // roundings of a cell moves a true value by at most 2^-1075 in the subnormal
 // range, so a sum S >= L*H*2^-1030 is exact to 5*2^-45 relative; that covers
 // pairs down to about 10^-599 * L*H.  Pairs below it (or non-finite) go on to
-// the extended tier's list.  No exponent bookkeeping: a step is the R cells,
-// the hand-off shuffles and the table loads.
+// the extended tier's list; a multi-tile pair goes there as soon as the mass on
+// a tile's border column (an upper bound of its final sum) is below half the
+// threshold, skipping its remaining tiles.  No exponent bookkeeping: a step is
+// the R cells, the hand-off shuffles and the table loads.
 //
 // Extended tier (EXT = true): an unrelated read far longer than its haplotype
 // lies thousands of decades below 1, beyond a pre-scaled double.  Every lane
@@ -359,6 +361,30 @@ struct Fp64Wavefront {
                 wnext = wpref;
             }
             __syncwarp();
+            if constexpr (MT && !EXT) {
+                // early hand-off to the extended tier: every path to the result crosses
+                // this tile's border column once and nothing on it exceeds 1, so the final
+                // sum is at most the border's mass, sum over rows of M + q*X^ (= M + I + D);
+                // below half the tier's threshold the sum would fail it at the end too
+                if (!last && !(GCP && !(beta > 0.0))) {
+                    const double qlast = __shfl_sync(kFullMask, qp, G - 1);
+                    double mass = 0.0;
+                    for (int j = t - 1; j < Hc; j += G) {
+                        const Border b = eout[j + kRowPad];
+                        mass += b.m + qlast * b.x;
+                    }
+#pragma unroll
+                    for (int d = 16; d >= 1; d >>= 1) mass += __shfl_xor_sync(kFullMask, mass, d);
+                    if (mass < 0.5 * scaled_tier_threshold(L, H)) {  // warp-uniform: one pair per warp
+                        if (valid && t == 0) {
+                            const int cls = fp64_class(L);
+                            const unsigned long long slot = atomicAdd(ext.count + cls, 1ull);
+                            ext.base[ext.off[cls] + (long long)slot] = task;
+                        }
+                        break;  // rlane stays -1: no score and no second append below
+                    }
+                }
+            }
         }
         if (valid && t == rlane) {
             double res = -INFINITY;
