@@ -35,6 +35,9 @@ constexpr int kCtrExt = kMaxBuckets + kFp64Classes;
 constexpr int kCtrTaskScaled = kMaxBuckets + 2 * kFp64Classes;
 constexpr int kCtrTaskExt = kMaxBuckets + 3 * kFp64Classes;
 constexpr int kCtrTotal = kMaxBuckets + 4 * kFp64Classes;
+// multi-tile FP64 pairs up to which the two tiers run fused (about one round of
+// resident warps of that class's kernel on 148 SMs)
+constexpr int64_t kFuseMaxPairs = 2048;
 
 std::vector<TileRule> engine_default_rules() {
     // Tile per read-length bucket for the persistent engine, measured on a B200
@@ -206,8 +209,10 @@ pairhmm_status_t Engine::init() {
     for (int c = 0; c < kFp64Classes; ++c)
         for (const bool gcp : {false, true})
             for (const bool ext : {false, true})
-                PHMM_CUDA(cudaFuncSetAttribute(fp64_kernel(c, gcp, ext), cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                               (int)fp64_smem_bytes(c, ext)));
+                for (const bool fuse : {false, true})
+                    PHMM_CUDA(cudaFuncSetAttribute(fp64_kernel(c, gcp, ext, fuse),
+                                                   cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                   (int)fp64_smem_bytes(c, ext)));
 
     // probability table p(q) = float(10^(-q/10)) (gpuworker.cuh:473-486)
     float table[128];
@@ -713,14 +718,22 @@ pairhmm_status_t Engine::enqueue_pipeline(const pairhmm_batch_t& in, const Batch
     } else {
         // stage 2: FP64 pass over flagged pairs (FP32 underflow, or degenerate alpha):
         // per length class the scaled tier, then on the same stream the extended
-        // tier over the pairs the scaled tier handed on; only the last class uses
+        // tier over the pairs the scaled tier handed on (for the multi-tile class of
+        // a small batch, inside the scaled tier's launch); only the last class uses
         // the border scratch (the two tiers of a class run in turn, so they share it)
         const ExtList ext{rescue_ext_.as<Task>(), rescue_off_.as<long long>(), counters + kCtrExt};
+        // a few long pairs (at most a round of resident warps): the multi-tile scaled tier
+        // runs a pair's extended form right after it in the same warp, so the batch waits
+        // for one pass instead of two
+        const bool fuse_mt = x.class_pairs[kFp64Classes - 1] <= kFuseMaxPairs;
         for (int c = 0; c < kFp64Classes; ++c) {
             if (x.class_pairs[c] == 0) continue;
             const cudaStream_t sc = next_stream();
+            const bool fuse = fuse_mt && c == kFp64Classes - 1;
             for (const bool tier_ext : {false, true}) {
+                if (tier_ext && fuse) continue;
                 Fp64LaunchArgs fa{};
+                fa.fuse = fuse && !tier_ext;
                 fa.view = v;
                 fa.cls = c;
                 fa.gcp = opts_.gcp != 0;

@@ -34,6 +34,7 @@ struct Fp64LaunchArgs {
     bool gcp;                        // gcp mode kernel
     bool ext;                        // extended-range tier (per-lane exponents)
     ExtList ext_list;                // scaled tier: where pairs beyond its range go
+    bool fuse = false;               // multi-tile scaled tier: run the extended form in the same warp
     const Task* items;               // that class's rescue list
     const unsigned long long* count; // number of items (device)
     unsigned long long* counter;     // task counter
@@ -68,7 +69,7 @@ const ConfigInfo* find_fp32_config(int G, int R, bool multi_tile, bool packed = 
 cudaError_t launch_fp64_rescue(const Fp64LaunchArgs& a);
 size_t fp64_smem_bytes(int cls, bool ext);
 size_t fp64_scratch_bytes_per_row(int cls, bool ext);  // per warp, per border row
-const void* fp64_kernel(int cls, bool gcp, bool ext);
+const void* fp64_kernel(int cls, bool gcp, bool ext, bool fuse = false);
 int fp64_per_warp(int cls);
 
 // Preparation kernels.

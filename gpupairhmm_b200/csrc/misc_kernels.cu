@@ -60,7 +60,20 @@ static_assert(W64c0<true>::T == kFp64ClassMax[0] && W64c1<true>::T == kFp64Class
                   W64c4<true>::T == kFp64ClassMax[4] && W64c5<true>::T == kFp64ClassMax[5],
               "class bounds follow the tiles");
 
+// The multi-tile class's scaled tier runs the extended form of a pair right
+// after it in the same warp when the pair needs it, so the border ring and the
+// scratch rows are sized for the extended form's 32-byte rows.
 template <class W>
+using Fp64ExtOf = Fp64Wavefront<W::G_, W::R_, W::kMT, W::kGCP, true>;
+template <class W>
+constexpr size_t fp64_ring_entry() { return W::kMT ? sizeof(Border64) : sizeof(typename W::Border); }
+
+
+// FUSE (multi-tile scaled tier): a pair that needs the extended tier runs it
+// right away in the same warp, instead of waiting in the extended tier's list
+// for a launch of its own; for batches of a few long regions (one long pair is
+// a long serial wavefront) that takes the second pass off their latency.
+template <class W, bool FUSE>
 __global__ void __launch_bounds__(kBlockThreads, W::kMinCtas)
 fp64_rescue_kernel(DevView v, const Task* __restrict__ items, const unsigned long long* count,
                    unsigned long long* counter, void* scratch, int64_t rows, ExtList ext) {
@@ -70,13 +83,14 @@ fp64_rescue_kernel(DevView v, const Task* __restrict__ items, const unsigned lon
     const int warp = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
     double2* wtab = smem64 + 32 + warp * W::kTableDouble2;
-    Border* ring = reinterpret_cast<Border*>(smem64 + 32 + kWarpsPerBlock * W::kTableDouble2) + warp * W::kRing;
+    char* ring_bytes = reinterpret_cast<char*>(smem64 + 32 + kWarpsPerBlock * W::kTableDouble2) +
+                       (size_t)warp * W::kRing * fp64_ring_entry<W>();
     for (int i = threadIdx.x; i < 128; i += blockDim.x) ph[i] = v.ph2pr[i];
     __syncthreads();
     const unsigned long long n = *count;
     const unsigned long long ntasks = (n + W::NG - 1) / W::NG;
     const long long gwarp = (long long)blockIdx.x * kWarpsPerBlock + warp;
-    Border* wscratch = scratch ? static_cast<Border*>(scratch) + gwarp * rows : nullptr;
+    char* wscratch = scratch ? static_cast<char*>(scratch) + (size_t)gwarp * rows * fp64_ring_entry<W>() : nullptr;
     while (true) {
         unsigned long long x = 0;
         if (lane == 0) x = atomicAdd(counter, 1ull);
@@ -84,14 +98,24 @@ fp64_rescue_kernel(DevView v, const Task* __restrict__ items, const unsigned lon
         if (x >= ntasks) break;
         const unsigned long long first = x * W::NG;
         const int ntask = (int)((n - first) < (unsigned long long)W::NG ? (n - first) : W::NG);
-        W::run(v, items + first, ntask, ph, wtab, ring, wscratch, rows, ext);
+        const bool to_ext = W::run(v, items + first, ntask, ph, wtab, reinterpret_cast<Border*>(ring_bytes),
+                                   reinterpret_cast<Border*>(wscratch), rows, ext, FUSE);
+        if constexpr (FUSE) {
+            if (to_ext) {  // warp-uniform: one pair per warp
+                using WE = Fp64ExtOf<W>;
+                __syncwarp();
+                WE::run(v, items + first, ntask, ph, wtab, reinterpret_cast<typename WE::Border*>(ring_bytes),
+                        reinterpret_cast<typename WE::Border*>(wscratch), rows, ext, false);
+                if (lane == 0) atomicAdd(ext.count + (kFp64Classes - 1), 1ull);  // counted with the extended tier
+            }
+        }
     }
 }
 
 template <class W>
 size_t fp64_smem_for() {
     return (32 + (size_t)kWarpsPerBlock * W::kTableDouble2) * sizeof(double2) +
-           (size_t)kWarpsPerBlock * W::kRing * sizeof(typename W::Border);
+           (size_t)kWarpsPerBlock * W::kRing * fp64_ring_entry<W>();
 }
 
 // gcp-mode twins of the class kernels (same tiles, eps/beta per read)
@@ -121,30 +145,54 @@ struct WithGcp<Fp64Wavefront<G, R, MT, false, EXT>> {
 // the gcp twin has the same tables and ring, so the same shared memory
 size_t fp64_smem_bytes(int cls, bool ext) { PHMM_FP64_DISPATCH(cls, ext, return fp64_smem_for<W>()); }
 // one border buffer per warp, shared by all tile boundaries of its pair
-size_t fp64_scratch_bytes_per_row(int cls, bool ext) {
-    if (cls != kFp64Classes - 1) return 0;
-    return ext ? sizeof(Border64) : sizeof(Border64S);
+size_t fp64_scratch_bytes_per_row(int cls, bool) {
+    return cls == kFp64Classes - 1 ? sizeof(Border64) : 0;  // both forms of the multi-tile class
 }
-const void* fp64_kernel(int cls, bool gcp, bool ext) {
-    PHMM_FP64_DISPATCH(cls, ext,
-                       return gcp ? reinterpret_cast<const void*>(&fp64_rescue_kernel<typename WithGcp<W>::type>)
-                                  : reinterpret_cast<const void*>(&fp64_rescue_kernel<W>));
+// the kernel of a class and tier; fuse picks the multi-tile scaled tier's fused form
+template <class W>
+const void* fp64_kernel_of(bool gcp, bool fuse) {
+    using WG = typename WithGcp<W>::type;
+    if constexpr (W::kMT && !W::kEXT) {
+        if (fuse)
+            return gcp ? reinterpret_cast<const void*>(&fp64_rescue_kernel<WG, true>)
+                       : reinterpret_cast<const void*>(&fp64_rescue_kernel<W, true>);
+    }
+    return gcp ? reinterpret_cast<const void*>(&fp64_rescue_kernel<WG, false>)
+               : reinterpret_cast<const void*>(&fp64_rescue_kernel<W, false>);
+}
+const void* fp64_kernel(int cls, bool gcp, bool ext, bool fuse) {
+    PHMM_FP64_DISPATCH(cls, ext, return fp64_kernel_of<W>(gcp, fuse));
 }
 int fp64_per_warp(int cls) { PHMM_FP64_DISPATCH(cls, true, return W::NG); }
+
+template <class K>
+cudaError_t fp64_launch_as(const Fp64LaunchArgs& a, void* scr, size_t smem) {
+    K::launch(a, scr, smem);
+    return cudaGetLastError();
+}
+template <class W, bool FUSE>
+struct Fp64Launch {
+    static void launch(const Fp64LaunchArgs& a, void* scr, size_t smem) {
+        fp64_rescue_kernel<W, FUSE><<<a.grid, kBlockThreads, smem, a.stream>>>(a.view, a.items, a.count, a.counter,
+                                                                              scr, a.rows, a.ext_list);
+    }
+};
+template <class W>
+cudaError_t fp64_launch_of(const Fp64LaunchArgs& a, void* scr, size_t smem) {
+    using WG = typename WithGcp<W>::type;
+    if constexpr (W::kMT && !W::kEXT) {
+        if (a.fuse)
+            return a.gcp ? fp64_launch_as<Fp64Launch<WG, true>>(a, scr, smem)
+                         : fp64_launch_as<Fp64Launch<W, true>>(a, scr, smem);
+    }
+    return a.gcp ? fp64_launch_as<Fp64Launch<WG, false>>(a, scr, smem)
+                 : fp64_launch_as<Fp64Launch<W, false>>(a, scr, smem);
+}
 
 cudaError_t launch_fp64_rescue(const Fp64LaunchArgs& a) {
     void* scr = a.cls == kFp64Classes - 1 ? a.scratch : nullptr;
     const size_t smem = fp64_smem_bytes(a.cls, a.ext);
-    if (a.gcp) {
-        PHMM_FP64_DISPATCH(a.cls, a.ext,
-                           (fp64_rescue_kernel<typename WithGcp<W>::type><<<a.grid, kBlockThreads, smem, a.stream>>>(
-                                a.view, a.items, a.count, a.counter, scr, a.rows, a.ext_list));
-                           return cudaGetLastError());
-    }
-    PHMM_FP64_DISPATCH(a.cls, a.ext,
-                       (fp64_rescue_kernel<W><<<a.grid, kBlockThreads, smem, a.stream>>>(
-                            a.view, a.items, a.count, a.counter, scr, a.rows, a.ext_list));
-                       return cudaGetLastError());
+    PHMM_FP64_DISPATCH(a.cls, a.ext, return fp64_launch_of<W>(a, scr, smem));
 }
 
 // ---------------------------------------------------------------- preparation

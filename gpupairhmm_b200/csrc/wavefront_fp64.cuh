@@ -12,7 +12,8 @@
 // pairs down to about 10^-599 * L*H.  Pairs below it (or non-finite) go on to
 // the extended tier's list; a multi-tile pair goes there as soon as the mass on
 // a tile's border column (an upper bound of its final sum) is below half the
-// threshold, skipping its remaining tiles.  No exponent bookkeeping: a step is
+// threshold, skipping its remaining tiles.  With fuse (multi-tile class, small
+// batches) the pair is not listed: the same warp runs its extended form next.  No exponent bookkeeping: a step is
 // the R cells, the hand-off shuffles and the table loads.
 //
 // Extended tier (EXT = true): an unrelated read far longer than its haplotype
@@ -104,6 +105,8 @@ struct Fp64Wavefront {
     static_assert(!MT || G == 32, "multi-tile FP64 runs one pair per warp");
     static constexpr int NG = 32 / G;
     static constexpr int T = G * R;
+    static constexpr int G_ = G, R_ = R;
+    static constexpr bool kMT = MT, kGCP = GCP, kEXT = EXT;
     static constexpr int Q = R / 2;                   // double2 per thread per table row
     static constexpr int kTableDouble2 = 5 * Q * 32;  // per warp
     static constexpr int kRing = 32;
@@ -126,8 +129,10 @@ struct Fp64Wavefront {
     // tasks: the warp's ntask (<= NG) items.  wtab: this warp's lambda table;
     // ring: kRing shared entries (MT); scratch: this warp's rows border entries.
     // ext: the extended tier's lists (scaled tier only).
-    __device__ static void run(const DevView& v, const Task* tasks, int ntask, const float* ph, double2* wtab,
-                               Border* ring, Border* scratch, int64_t rows, const ExtList& ext) {
+    // fuse (multi-tile scaled tier only): a pair that needs the extended tier is not
+    // appended to its list; run returns true and the caller runs the extended form
+    __device__ static bool run(const DevView& v, const Task* tasks, int ntask, const float* ph, double2* wtab,
+                               Border* ring, Border* scratch, int64_t rows, const ExtList& ext, bool fuse) {
         const int lane = threadIdx.x & 31;
         const int grp = lane / G;
         const int t = lane - grp * G;
@@ -376,30 +381,35 @@ struct Fp64Wavefront {
 #pragma unroll
                     for (int d = 16; d >= 1; d >>= 1) mass += __shfl_xor_sync(kFullMask, mass, d);
                     if (mass < 0.5 * scaled_tier_threshold(L, H)) {  // warp-uniform: one pair per warp
+                        if (fuse) return valid;
                         if (valid && t == 0) {
                             const int cls = fp64_class(L);
                             const unsigned long long slot = atomicAdd(ext.count + cls, 1ull);
                             ext.base[ext.off[cls] + (long long)slot] = task;
                         }
-                        break;  // rlane stays -1: no score and no second append below
+                        return false;  // no score: the extended tier writes it
                     }
                 }
             }
         }
+        // scaled tier: a sum too small (or not finite) for the fixed scale goes on to
+        // the extended tier, which overwrites the score
+        const bool to_ext = !EXT && valid && t == rlane && !(acc >= scaled_tier_threshold(L, H) && acc <= DBL_MAX) &&
+                            !(GCP && !(beta > 0.0));
         if (valid && t == rlane) {
             double res = -INFINITY;
             if (acc > 0.0)
                 res = log10(acc) - (double)eacc * 0.30102999566398119521 - log10((double)kScale) - log10(beta);
             if (GCP && !(beta > 0.0)) res = NAN;
             v.scores[task.out] = (float)res;
-            // scaled tier: a sum too small (or not finite) for the fixed scale goes on
-            // to the extended tier, which overwrites the score
-            if (!EXT && !(acc >= scaled_tier_threshold(L, H) && acc <= DBL_MAX) && !(GCP && !(beta > 0.0))) {
+            if (to_ext && !fuse) {
                 const int cls = fp64_class(L);
                 const unsigned long long slot = atomicAdd(ext.count + cls, 1ull);
                 ext.base[ext.off[cls] + (long long)slot] = task;
             }
         }
+        if (MT && !EXT && fuse) return __any_sync(kFullMask, to_ext);
+        return false;
     }
 };
 

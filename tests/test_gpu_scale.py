@@ -70,6 +70,26 @@ def test_fp64_tiers_split_by_range(engine):
     assert_log10_close(got, want, what="tiers")
 
 
+def test_fused_and_separate_fp64_tiers_agree_bitwise(engine):
+    """Up to 2,048 multi-tile pairs in a batch, the FP64 scaled tier runs a
+    pair's extended form right after it in the same warp; above that the
+    extended tier is a launch of its own.  A batch of 40 long-read regions
+    (2,560 multi-tile pairs: separate launches) gives every region's scores
+    bitwise as that region computed alone (64 pairs: fused)."""
+    from gpupairhmm_b200 import replicas
+    b = synth.config3(seed=505, regions=40)
+    got = engine.compute(b)
+    separate_ext = engine.stats().rescued_ext
+    assert separate_ext > 0
+    po = replicas.pair_offsets(b)
+    fused_ext = 0
+    for r in range(b.num_records):
+        alone = engine.compute(b.select_records(r, r + 1))
+        fused_ext += engine.stats().rescued_ext
+        np.testing.assert_array_equal(alone, got[po[r]:po[r + 1]])
+    assert fused_ext == separate_ext  # the same pairs take the extended form either way
+
+
 def test_serving_matches_batch_on_long_and_stress_regions(engine):
     """Regions of both heavy configurations through the serving queue give the
     batch call's scores bitwise."""
