@@ -53,12 +53,11 @@ void ServingQueue::stats(pairhmm_serving_stats_t* out) {
 int64_t ServingQueue::estimate_device_bytes(const Region& r) {
     // inputs (4 byte arrays + haplotypes), packed copies, work items, rescue
     // list and scores, plus the per-read/per-haplotype index arrays
-    const int64_t reads = (int64_t)r.read_len.size(), haps = (int64_t)r.hap_len.size();
     int64_t pos = 0, hb = 0;
-    for (int32_t L : r.read_len) pos += (L + 3) & ~3;
-    for (int32_t H : r.hap_len) hb += (H + 15) & ~15;
-    return 4 * (int64_t)r.read_bases.size() + 2 * (int64_t)r.hap_bases.size() + 4 * pos + hb +
-           r.pairs * (16 + 16 + 4) + reads * 32 + haps * 24 + 4096;
+    for (int64_t i = 0; i < r.reads; ++i) pos += (r.read_len()[i] + 3) & ~3;
+    for (int64_t h = 0; h < r.haps; ++h) hb += (r.hap_len()[h] + 15) & ~15;
+    return 4 * r.read_bytes + 2 * r.hap_bytes + 4 * pos + hb + r.pairs * (16 + 16 + 4) + r.reads * 32 +
+           r.haps * 24 + 4096;
 }
 
 pairhmm_status_t ServingQueue::prepare(const pairhmm_batch_t& b, std::shared_ptr<Region>& out,
@@ -70,38 +69,43 @@ pairhmm_status_t ServingQueue::prepare(const pairhmm_batch_t& b, std::shared_ptr
     const pairhmm_status_t st = Engine::scan_inputs(b, x, err, gcp);
     if (st != PAIRHMM_OK) return st;
     auto r = std::make_shared<Region>();
-    r->rpr.assign(b.reads_per_record, b.reads_per_record + b.num_records);
-    r->hpr.assign(b.haps_per_record, b.haps_per_record + b.num_records);
-    r->read_len.assign(b.read_lengths, b.read_lengths + x.num_reads);
-    r->hap_len.assign(b.hap_lengths, b.hap_lengths + x.num_haps);
-    // compact copy: each read/haplotype stored back to back
-    r->read_off.resize(x.num_reads);
-    r->hap_off.resize(x.num_haps);
-    int64_t total = 0;
+    r->records = b.num_records;
+    r->reads = x.num_reads;
+    r->haps = x.num_haps;
+    r->gcp = gcp;
     int32_t max_read_len = 0;
     for (int64_t i = 0; i < x.num_reads; ++i) {
-        r->read_off[i] = total;
-        total += b.read_lengths[i];
+        r->read_bytes += b.read_lengths[i];
         max_read_len = std::max(max_read_len, b.read_lengths[i]);
     }
-    r->read_bases.resize(total);
-    r->bq.resize(total);
-    r->iq.resize(total);
-    r->dq.resize(total);
-    if (gcp) r->gq.resize(total);
-    for (int64_t i = 0; i < x.num_reads; ++i) {
-        const int64_t o = b.read_offsets[i], d = r->read_off[i], L = b.read_lengths[i];
-        std::memcpy(&r->read_bases[d], b.read_bases + o, L);
-        std::memcpy(&r->bq[d], b.base_quals + o, L);
-        std::memcpy(&r->iq[d], b.ins_quals + o, L);
-        std::memcpy(&r->dq[d], b.del_quals + o, L);
-        if (gcp) std::memcpy(&r->gq[d], b.gcp_quals + o, L);
+    for (int64_t h = 0; h < x.num_haps; ++h) r->hap_bytes += b.hap_lengths[h];
+    const int64_t ints = 2 * r->records + r->reads + r->haps;
+    r->data.reset(new uint8_t[(size_t)std::max<int64_t>(4 * ints + (gcp ? 5 : 4) * r->read_bytes + r->hap_bytes, 1)]);
+    int32_t* ip = reinterpret_cast<int32_t*>(r->data.get());
+    auto put = [](void* dst, const void* src, int64_t bytes) {
+        if (bytes > 0) std::memcpy(dst, src, (size_t)bytes);
+    };
+    put(ip, b.reads_per_record, 4 * r->records);
+    put(ip + r->records, b.haps_per_record, 4 * r->records);
+    put(ip + 2 * r->records, b.read_lengths, 4 * r->reads);
+    put(ip + 2 * r->records + r->reads, b.hap_lengths, 4 * r->haps);
+    // compact copy: each read/haplotype stored back to back
+    uint8_t* rp = r->data.get() + 4 * ints;
+    const int64_t rbytes = r->read_bytes;
+    for (int64_t i = 0, d = 0; i < x.num_reads; ++i) {
+        const int64_t o = b.read_offsets[i], L = b.read_lengths[i];
+        put(rp + d, b.read_bases + o, L);
+        put(rp + rbytes + d, b.base_quals + o, L);
+        put(rp + 2 * rbytes + d, b.ins_quals + o, L);
+        put(rp + 3 * rbytes + d, b.del_quals + o, L);
+        if (gcp) put(rp + 4 * rbytes + d, b.gcp_quals + o, L);
+        d += L;
     }
-    total = 0;
-    for (int64_t h = 0; h < x.num_haps; ++h) { r->hap_off[h] = total; total += b.hap_lengths[h]; }
-    r->hap_bases.resize(total);
-    for (int64_t h = 0; h < x.num_haps; ++h)
-        std::memcpy(&r->hap_bases[r->hap_off[h]], b.hap_bases + b.hap_offsets[h], b.hap_lengths[h]);
+    uint8_t* hp = rp + (gcp ? 5 : 4) * rbytes;
+    for (int64_t h = 0, d = 0; h < x.num_haps; ++h) {
+        put(hp + d, b.hap_bases + b.hap_offsets[h], b.hap_lengths[h]);
+        d += b.hap_lengths[h];
+    }
     r->pairs = x.num_pairs;
     r->heavy = max_read_len > single_tile_max_;
     r->device_bytes = estimate_device_bytes(*r);
@@ -183,10 +187,9 @@ void ServingQueue::worker(int slot) {
     Engine& eng = *engines_[slot];
     std::deque<std::shared_ptr<Region>>& queue = slot < kLightSlots ? light_ : heavy_;
     // merge buffers live as long as the slot: a batch maps no new memory once
-    // they have grown to the slot's usual size
-    std::vector<int32_t> rpr, hpr, rl, hl;
-    std::vector<int64_t> ro, ho;
-    std::vector<uint8_t> rb, bq, iq, dq, gq, hb;
+    // they have grown to the slot's usual size (uninitialised: every byte is
+    // written by the merge)
+    MergeBuf m_rpr, m_hpr, m_rl, m_hl, m_ro, m_ho, m_rb, m_bq, m_iq, m_dq, m_gq, m_hb;
     std::vector<float> scores;
     for (;;) {
         std::vector<std::shared_ptr<Region>> take;
@@ -214,43 +217,77 @@ void ServingQueue::worker(int slot) {
         }
         if (more) cv_work_.notify_all();
         // merge the regions into one batch
-        for (auto* v : {&rpr, &hpr, &rl, &hl}) v->clear();
-        ro.clear();
-        ho.clear();
-        for (auto* v : {&rb, &bq, &iq, &dq, &gq, &hb}) v->clear();
+        int64_t nrec = 0, nreads = 0, nhaps = 0, rbytes = 0, hbytes = 0;
+        bool gcp = false;
         for (const auto& r : take) {
-            const int64_t rbase = (int64_t)rb.size(), hbase = (int64_t)hb.size();
-            rpr.insert(rpr.end(), r->rpr.begin(), r->rpr.end());
-            hpr.insert(hpr.end(), r->hpr.begin(), r->hpr.end());
-            rl.insert(rl.end(), r->read_len.begin(), r->read_len.end());
-            hl.insert(hl.end(), r->hap_len.begin(), r->hap_len.end());
-            for (int64_t o : r->read_off) ro.push_back(rbase + o);
-            for (int64_t o : r->hap_off) ho.push_back(hbase + o);
-            rb.insert(rb.end(), r->read_bases.begin(), r->read_bases.end());
-            bq.insert(bq.end(), r->bq.begin(), r->bq.end());
-            iq.insert(iq.end(), r->iq.begin(), r->iq.end());
-            dq.insert(dq.end(), r->dq.begin(), r->dq.end());
-            gq.insert(gq.end(), r->gq.begin(), r->gq.end());
-            hb.insert(hb.end(), r->hap_bases.begin(), r->hap_bases.end());
-            // the merged copy is all the batch needs: give the region's input copy back now
-            // rather than when it is drained (a client that drains late would otherwise hold
-            // every input it submitted meanwhile)
-            r->release_inputs();
+            nrec += r->records;
+            nreads += r->reads;
+            nhaps += r->haps;
+            rbytes += r->read_bytes;
+            hbytes += r->hap_bytes;
+            gcp = gcp || r->gcp;
+        }
+        int32_t* rpr = m_rpr.get<int32_t>(nrec);
+        int32_t* hpr = m_hpr.get<int32_t>(nrec);
+        int32_t* rl = m_rl.get<int32_t>(nreads);
+        int32_t* hl = m_hl.get<int32_t>(nhaps);
+        int64_t* ro = m_ro.get<int64_t>(nreads);
+        int64_t* ho = m_ho.get<int64_t>(nhaps);
+        uint8_t* rb = m_rb.get<uint8_t>(rbytes);
+        uint8_t* bq = m_bq.get<uint8_t>(rbytes);
+        uint8_t* iq = m_iq.get<uint8_t>(rbytes);
+        uint8_t* dq = m_dq.get<uint8_t>(rbytes);
+        uint8_t* gq = gcp ? m_gq.get<uint8_t>(rbytes) : nullptr;
+        uint8_t* hb = m_hb.get<uint8_t>(hbytes);
+        {
+            int64_t g = 0, i = 0, h = 0, rp = 0, hp = 0;
+            auto put = [](void* dst, const void* src, int64_t bytes) {
+                if (bytes > 0) std::memcpy(dst, src, (size_t)bytes);
+            };
+            for (const auto& r : take) {
+                put(rpr + g, r->rpr(), 4 * r->records);
+                put(hpr + g, r->hpr(), 4 * r->records);
+                put(rl + i, r->read_len(), 4 * r->reads);
+                put(hl + h, r->hap_len(), 4 * r->haps);
+                for (int64_t k = 0, o = rp; k < r->reads; ++k) {
+                    ro[i + k] = o;
+                    o += r->read_len()[k];
+                }
+                for (int64_t k = 0, o = hp; k < r->haps; ++k) {
+                    ho[h + k] = o;
+                    o += r->hap_len()[k];
+                }
+                put(rb + rp, r->read_part(0), r->read_bytes);
+                put(bq + rp, r->read_part(1), r->read_bytes);
+                put(iq + rp, r->read_part(2), r->read_bytes);
+                put(dq + rp, r->read_part(3), r->read_bytes);
+                if (gcp) put(gq + rp, r->read_part(4), r->read_bytes);
+                put(hb + hp, r->hap_bases(), r->hap_bytes);
+                g += r->records;
+                i += r->reads;
+                h += r->haps;
+                rp += r->read_bytes;
+                hp += r->hap_bytes;
+                // the merged copy is all the batch needs: give the region's input copy back
+                // now rather than when it is drained (a client that drains late would
+                // otherwise hold every input it submitted meanwhile)
+                r->release_inputs();
+            }
         }
         pairhmm_batch_t b{};
-        b.num_records = (int64_t)rpr.size();
-        b.reads_per_record = rpr.data();
-        b.haps_per_record = hpr.data();
-        b.read_bases = rb.data();
-        b.base_quals = bq.data();
-        b.ins_quals = iq.data();
-        b.del_quals = dq.data();
-        b.gcp_quals = gq.empty() ? nullptr : gq.data();
-        b.read_offsets = ro.data();
-        b.read_lengths = rl.data();
-        b.hap_bases = hb.data();
-        b.hap_offsets = ho.data();
-        b.hap_lengths = hl.data();
+        b.num_records = nrec;
+        b.reads_per_record = rpr;
+        b.haps_per_record = hpr;
+        b.read_bases = rb;
+        b.base_quals = bq;
+        b.ins_quals = iq;
+        b.del_quals = dq;
+        b.gcp_quals = gq;
+        b.read_offsets = ro;
+        b.read_lengths = rl;
+        b.hap_bases = hb;
+        b.hap_offsets = ho;
+        b.hap_lengths = hl;
         int64_t total_pairs = 0;
         for (const auto& r : take) total_pairs += r->pairs;
         scores.resize((size_t)std::max<int64_t>(total_pairs, 1));

@@ -15,6 +15,7 @@
 // them and a long region waits for at most one batch of long ones.
 #pragma once
 
+#include <algorithm>
 #include <chrono>
 #include <condition_variable>
 #include <cstdint>
@@ -52,9 +53,12 @@ public:
 private:
     struct Region {
         uint64_t ticket = 0;
-        std::vector<int32_t> rpr, hpr, read_len, hap_len;
-        std::vector<int64_t> read_off, hap_off;
-        std::vector<uint8_t> read_bases, bq, iq, dq, gq, hap_bases;  // gq: gcp mode only
+        // the region's inputs in one allocation: per record R and H, read and
+        // haplotype lengths (int32), then the read bases, base/ins/del (and in gcp
+        // mode gcp) qualities and the haplotype bases, each packed back to back
+        std::unique_ptr<uint8_t[]> data;
+        int64_t records = 0, reads = 0, haps = 0, read_bytes = 0, hap_bytes = 0;
+        bool gcp = false;
         int64_t pairs = 0;
         int64_t device_bytes = 0;
         bool heavy = false;  // has a read beyond the largest single tile
@@ -63,12 +67,31 @@ private:
         bool done = false;
         pairhmm_status_t status = PAIRHMM_OK;
         std::string error;
+
+        const int32_t* rpr() const { return reinterpret_cast<const int32_t*>(data.get()); }
+        const int32_t* hpr() const { return rpr() + records; }
+        const int32_t* read_len() const { return hpr() + records; }
+        const int32_t* hap_len() const { return read_len() + reads; }
+        const uint8_t* read_part(int k) const {  // 0 bases, 1 base, 2 ins, 3 del, 4 gcp quals
+            return data.get() + 4 * (2 * records + reads + haps) + k * read_bytes;
+        }
+        const uint8_t* hap_bases() const { return read_part(gcp ? 5 : 4); }
         // after the merge only the counts, pairs and results are used
-        void release_inputs() {
-            for (auto* v : {&rpr, &hpr, &read_len, &hap_len}) std::vector<int32_t>().swap(*v);
-            std::vector<int64_t>().swap(read_off);
-            std::vector<int64_t>().swap(hap_off);
-            for (auto* v : {&read_bases, &bq, &iq, &dq, &gq, &hap_bases}) std::vector<uint8_t>().swap(*v);
+        void release_inputs() { data.reset(); }
+    };
+
+    // reusable, uninitialised host buffer of a slot's merged batch
+    struct MergeBuf {
+        std::unique_ptr<uint8_t[]> p;
+        size_t cap = 0;
+        template <class T>
+        T* get(int64_t n) {
+            const size_t bytes = (size_t)std::max<int64_t>(n, 1) * sizeof(T);
+            if (bytes > cap) {
+                cap = bytes + bytes / 4;
+                p.reset(new uint8_t[cap]);
+            }
+            return reinterpret_cast<T*>(p.get());
         }
     };
 
