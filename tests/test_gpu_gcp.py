@@ -103,3 +103,30 @@ def test_gcp_mode_rejections():
     e.close()
     with pytest.raises(g.PairHMMError):
         g.Engine(mode=g.MODE_PLAIN, gcp=True)
+
+
+def test_gcp_serving_matches_batch_call(gcp_engine):
+    """gcp mode through the serving queue (the regions' gcp qualities travel with
+    their other arrays into the merged batch): scores equal the batch call's
+    bitwise, for short and multi-tile regions submitted together."""
+    regions = [with_gcp(synth.config1(seed=600 + i, regions=1), 700 + i) for i in range(6)] + \
+              [with_gcp(synth.config3(seed=610, regions=1), 710)]
+    want = [gcp_engine.compute(r) for r in regions]
+    e = g.Engine(gcp=True)
+    tickets = e.submit_many(regions)
+    for t, r, w in zip(tickets, regions, want):
+        np.testing.assert_array_equal(e.drain(t, r.num_pairs, timeout_ms=120000), w)
+    e.close()
+
+
+def test_gcp_fused_and_separate_fp64_tiers_agree_bitwise(gcp_engine):
+    """gcp mode, multi-tile FP64 pairs: a 40-region long-read batch (2,560
+    multi-tile pairs, separate tier launches) gives each region's scores
+    bitwise as the region alone (64 pairs, tiers fused in one launch)."""
+    from gpupairhmm_b200 import replicas
+    b = with_gcp(synth.config3(seed=620, regions=40), 720, lo=5, hi=41)
+    got = gcp_engine.compute(b)
+    assert gcp_engine.stats().rescued > 0
+    po = replicas.pair_offsets(b)
+    for r in range(b.num_records):
+        np.testing.assert_array_equal(gcp_engine.compute(b.select_records(r, r + 1)), got[po[r]:po[r + 1]])
