@@ -1,5 +1,7 @@
 #include <algorithm>
 #include <cstring>
+#include <new>
+#include <stdexcept>
 #include <string>
 
 #include "serving.hpp"
@@ -216,82 +218,94 @@ void ServingQueue::worker(int slot) {
             max_in_flight_ = std::max(max_in_flight_, ++in_flight_);
         }
         if (more) cv_work_.notify_all();
-        // merge the regions into one batch
-        int64_t nrec = 0, nreads = 0, nhaps = 0, rbytes = 0, hbytes = 0;
-        bool gcp = false;
-        for (const auto& r : take) {
-            nrec += r->records;
-            nreads += r->reads;
-            nhaps += r->haps;
-            rbytes += r->read_bytes;
-            hbytes += r->hap_bytes;
-            gcp = gcp || r->gcp;
-        }
-        int32_t* rpr = m_rpr.get<int32_t>(nrec);
-        int32_t* hpr = m_hpr.get<int32_t>(nrec);
-        int32_t* rl = m_rl.get<int32_t>(nreads);
-        int32_t* hl = m_hl.get<int32_t>(nhaps);
-        int64_t* ro = m_ro.get<int64_t>(nreads);
-        int64_t* ho = m_ho.get<int64_t>(nhaps);
-        uint8_t* rb = m_rb.get<uint8_t>(rbytes);
-        uint8_t* bq = m_bq.get<uint8_t>(rbytes);
-        uint8_t* iq = m_iq.get<uint8_t>(rbytes);
-        uint8_t* dq = m_dq.get<uint8_t>(rbytes);
-        uint8_t* gq = gcp ? m_gq.get<uint8_t>(rbytes) : nullptr;
-        uint8_t* hb = m_hb.get<uint8_t>(hbytes);
-        {
-            int64_t g = 0, i = 0, h = 0, rp = 0, hp = 0;
-            auto put = [](void* dst, const void* src, int64_t bytes) {
-                if (bytes > 0) std::memcpy(dst, src, (size_t)bytes);
-            };
+        // merge the regions into one batch and run it; a failure (host memory
+        // included: this thread has no caller to throw to) fails the batch's regions
+        pairhmm_status_t st = PAIRHMM_OK;
+        std::string batch_error;
+        try {
+            int64_t nrec = 0, nreads = 0, nhaps = 0, rbytes = 0, hbytes = 0;
+            bool gcp = false;
             for (const auto& r : take) {
-                put(rpr + g, r->rpr(), 4 * r->records);
-                put(hpr + g, r->hpr(), 4 * r->records);
-                put(rl + i, r->read_len(), 4 * r->reads);
-                put(hl + h, r->hap_len(), 4 * r->haps);
-                for (int64_t k = 0, o = rp; k < r->reads; ++k) {
-                    ro[i + k] = o;
-                    o += r->read_len()[k];
-                }
-                for (int64_t k = 0, o = hp; k < r->haps; ++k) {
-                    ho[h + k] = o;
-                    o += r->hap_len()[k];
-                }
-                put(rb + rp, r->read_part(0), r->read_bytes);
-                put(bq + rp, r->read_part(1), r->read_bytes);
-                put(iq + rp, r->read_part(2), r->read_bytes);
-                put(dq + rp, r->read_part(3), r->read_bytes);
-                if (gcp) put(gq + rp, r->read_part(4), r->read_bytes);
-                put(hb + hp, r->hap_bases(), r->hap_bytes);
-                g += r->records;
-                i += r->reads;
-                h += r->haps;
-                rp += r->read_bytes;
-                hp += r->hap_bytes;
-                // the merged copy is all the batch needs: give the region's input copy back
-                // now rather than when it is drained (a client that drains late would
-                // otherwise hold every input it submitted meanwhile)
-                r->release_inputs();
+                nrec += r->records;
+                nreads += r->reads;
+                nhaps += r->haps;
+                rbytes += r->read_bytes;
+                hbytes += r->hap_bytes;
+                gcp = gcp || r->gcp;
             }
+            int32_t* rpr = m_rpr.get<int32_t>(nrec);
+            int32_t* hpr = m_hpr.get<int32_t>(nrec);
+            int32_t* rl = m_rl.get<int32_t>(nreads);
+            int32_t* hl = m_hl.get<int32_t>(nhaps);
+            int64_t* ro = m_ro.get<int64_t>(nreads);
+            int64_t* ho = m_ho.get<int64_t>(nhaps);
+            uint8_t* rb = m_rb.get<uint8_t>(rbytes);
+            uint8_t* bq = m_bq.get<uint8_t>(rbytes);
+            uint8_t* iq = m_iq.get<uint8_t>(rbytes);
+            uint8_t* dq = m_dq.get<uint8_t>(rbytes);
+            uint8_t* gq = gcp ? m_gq.get<uint8_t>(rbytes) : nullptr;
+            uint8_t* hb = m_hb.get<uint8_t>(hbytes);
+            {
+                int64_t g = 0, i = 0, h = 0, rp = 0, hp = 0;
+                auto put = [](void* dst, const void* src, int64_t bytes) {
+                    if (bytes > 0) std::memcpy(dst, src, (size_t)bytes);
+                };
+                for (const auto& r : take) {
+                    put(rpr + g, r->rpr(), 4 * r->records);
+                    put(hpr + g, r->hpr(), 4 * r->records);
+                    put(rl + i, r->read_len(), 4 * r->reads);
+                    put(hl + h, r->hap_len(), 4 * r->haps);
+                    for (int64_t k = 0, o = rp; k < r->reads; ++k) {
+                        ro[i + k] = o;
+                        o += r->read_len()[k];
+                    }
+                    for (int64_t k = 0, o = hp; k < r->haps; ++k) {
+                        ho[h + k] = o;
+                        o += r->hap_len()[k];
+                    }
+                    put(rb + rp, r->read_part(0), r->read_bytes);
+                    put(bq + rp, r->read_part(1), r->read_bytes);
+                    put(iq + rp, r->read_part(2), r->read_bytes);
+                    put(dq + rp, r->read_part(3), r->read_bytes);
+                    if (gcp) put(gq + rp, r->read_part(4), r->read_bytes);
+                    put(hb + hp, r->hap_bases(), r->hap_bytes);
+                    g += r->records;
+                    i += r->reads;
+                    h += r->haps;
+                    rp += r->read_bytes;
+                    hp += r->hap_bytes;
+                    // the merged copy is all the batch needs: give the region's input copy back
+                    // now rather than when it is drained (a client that drains late would
+                    // otherwise hold every input it submitted meanwhile)
+                    r->release_inputs();
+                }
+            }
+            pairhmm_batch_t b{};
+            b.num_records = nrec;
+            b.reads_per_record = rpr;
+            b.haps_per_record = hpr;
+            b.read_bases = rb;
+            b.base_quals = bq;
+            b.ins_quals = iq;
+            b.del_quals = dq;
+            b.gcp_quals = gq;
+            b.read_offsets = ro;
+            b.read_lengths = rl;
+            b.hap_bases = hb;
+            b.hap_offsets = ho;
+            b.hap_lengths = hl;
+            int64_t total_pairs = 0;
+            for (const auto& r : take) total_pairs += r->pairs;
+            scores.resize((size_t)std::max<int64_t>(total_pairs, 1));
+            st = eng.compute_host(b, scores.data());
+            if (st != PAIRHMM_OK) batch_error = eng.last_error();
+        } catch (const std::bad_alloc&) {
+            st = PAIRHMM_ERR_OUT_OF_MEMORY;
+            batch_error = "host allocation failed while merging a batch";
+        } catch (const std::exception& e) {
+            st = PAIRHMM_ERR_CUDA;
+            batch_error = e.what();
         }
-        pairhmm_batch_t b{};
-        b.num_records = nrec;
-        b.reads_per_record = rpr;
-        b.haps_per_record = hpr;
-        b.read_bases = rb;
-        b.base_quals = bq;
-        b.ins_quals = iq;
-        b.del_quals = dq;
-        b.gcp_quals = gq;
-        b.read_offsets = ro;
-        b.read_lengths = rl;
-        b.hap_bases = hb;
-        b.hap_offsets = ho;
-        b.hap_lengths = hl;
-        int64_t total_pairs = 0;
-        for (const auto& r : take) total_pairs += r->pairs;
-        scores.resize((size_t)std::max<int64_t>(total_pairs, 1));
-        const pairhmm_status_t st = eng.compute_host(b, scores.data());
         const auto now = std::chrono::steady_clock::now();
         {
             std::lock_guard<std::mutex> lk(mu_);
@@ -300,8 +314,16 @@ void ServingQueue::worker(int slot) {
             int64_t off = 0;
             for (const auto& r : take) {
                 r->status = st;
-                if (st != PAIRHMM_OK) r->error = eng.last_error();
-                else r->scores.assign(scores.begin() + off, scores.begin() + off + r->pairs);
+                if (st != PAIRHMM_OK) {
+                    r->error = batch_error;
+                } else {
+                    try {
+                        r->scores.assign(scores.begin() + off, scores.begin() + off + r->pairs);
+                    } catch (const std::bad_alloc&) {
+                        r->status = PAIRHMM_ERR_OUT_OF_MEMORY;
+                        r->error = "host allocation failed for the region's scores";
+                    }
+                }
                 off += r->pairs;
                 r->t_done = now;
                 r->done = true;
