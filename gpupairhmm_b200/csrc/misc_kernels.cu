@@ -68,7 +68,6 @@ using Fp64ExtOf = Fp64Wavefront<W::G_, W::R_, W::kMT, W::kGCP, true>;
 template <class W>
 constexpr size_t fp64_ring_entry() { return W::kMT ? sizeof(Border64) : sizeof(typename W::Border); }
 
-
 // FUSE (multi-tile scaled tier): a pair that needs the extended tier runs it
 // right away in the same warp, instead of waiting in the extended tier's list
 // for a launch of its own; for batches of a few long regions (one long pair is
