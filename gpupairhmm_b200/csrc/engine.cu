@@ -1004,13 +1004,14 @@ pairhmm_status_t Engine::compute_host(const pairhmm_batch_t& b, float* scores) {
         PHMM_CUDA(cudaEventCreate(&span0_));
         PHMM_CUDA(cudaEventCreate(&span1_));
     }
-    // chunk boundaries: records in order, about equal pairs per chunk
+    // chunk boundaries: records in order, about equal pairs per chunk except the
+    // first, which is half a chunk (its index build and upload are not overlapped)
     std::vector<int64_t> bound{0};
     {
         int64_t acc = 0, next = 1;
         for (int64_t g = 0; g < b.num_records && (int)bound.size() < nchunks; ++g) {
             acc += (int64_t)std::max(b.reads_per_record[g], 0) * std::max(b.haps_per_record[g], 0);
-            if (acc * nchunks >= pairs * next && g + 1 < b.num_records) {
+            if (acc * (2 * nchunks - 1) >= pairs * (2 * next - 1) && g + 1 < b.num_records) {
                 bound.push_back(g + 1);
                 ++next;
             }
