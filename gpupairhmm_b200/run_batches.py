@@ -21,7 +21,7 @@ from . import synth
 
 CONFIGS = {
     "small": lambda n, seed: synth.config0(seed=seed, records=n or 64),
-    "uneven": lambda n, seed: synth.config1(seed=seed, regions=n or 20000),
+    "uneven": lambda n, seed, sigma=1.0: synth.config1(seed=seed, regions=n or 20000, sigma=sigma),
     "stress": lambda n, seed: synth.config2(seed=seed, regions=n or 5000),
     "long": lambda n, seed: synth.config3(seed=seed, regions=n or 2000),
 }
@@ -36,10 +36,12 @@ def main() -> None:
     ap.add_argument("--mode", choices=["engine", "plain"], default="engine")
     ap.add_argument("--pageable", action="store_true", help="pass pageable numpy arrays (default: page-locked)")
     ap.add_argument("--device", type=int, default=0)
+    ap.add_argument("--sigma", type=float, default=1.0,
+                    help="uneven configuration: sigma of the lognormal reads-per-region count")
     ap.add_argument("--chunks", type=int, default=1,
                     help="pipeline_chunks of the engine (1 = one pass, whose stage times add up; 0 = auto)")
     a = ap.parse_args()
-    batch = CONFIGS[a.config](a.regions, a.seed)
+    batch = CONFIGS[a.config](a.regions, a.seed, a.sigma) if a.config == "uneven" else CONFIGS[a.config](a.regions, a.seed)
     inputs = batch if a.pageable else batch.pin()
     with Engine(device=a.device, mode=MODE_PLAIN if a.mode == "plain" else MODE_ENGINE,
                 pipeline_chunks=a.chunks) as e:
