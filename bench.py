@@ -647,8 +647,8 @@ def run_ours(args, cfg, rank, world, local_rank):
             "roofline": {"bound": "fp32", "achieved": round(achieved, 3), "peak": round(peak, 3),
                          "unit": "TFLOP/s", "frac": round(achieved / peak, 4),
                          "traffic": (round(tpc * cells / n_fp32_launches) if tpc else None),
-                         "peak_source": "FFMA throughput measured in this run on this GPU (no FP32 entry in "
-                                        "the driver's peak file)",
+                         "peak_source": "FFMA throughput measured in this run on this GPU (MEASURED_PEAKS.json "
+                                        "has no FP32 entry)",
                          "flop_per_cell": FLOPS_PER_CELL,
                          # 11 algorithmic FLOP per cell in 5 FMA-pipe instructions (4 FFMA + 1 FMUL)
                          "instruction_mix_ceiling": round(FLOPS_PER_CELL / 10, 4),
